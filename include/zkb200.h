@@ -1,0 +1,179 @@
+/*
+ * zkb200.h — C ABI of the B200 polynomial-commitment library (libzkb200.so).
+ *
+ * The library is a drop-in for the ZirOS accelerator path of the Plonky3 STARK
+ * backend: coset NTT / low-degree extension, Poseidon2 Merkle commitment (MMCS)
+ * and FRI folding over BabyBear and Goldilocks.  Each entry point names the
+ * reference interface it replaces (paths relative to the ZirOS repository root).
+ *
+ * Conventions
+ *  - Field elements are canonical integers in [0, p): uint32_t for BabyBear,
+ *    uint64_t for Goldilocks.  Matrices are row-major (p3 RowMajorMatrix).
+ *  - Return status: ZKB_OK (0); ZKB_DECLINED (1) = "not accelerated, use the CPU
+ *    path" (the reference's `false` / `None`, e.g. zkf-metal/src/poseidon2/mod.rs:44-46);
+ *    negative = error.  The message of the last failure on the calling thread is
+ *    returned by zkb_last_error_message(), as zkf-ffi does
+ *    (zkf-ffi/src/lib.rs:49-60,165-171).
+ *  - Entry points without a suffix take HOST pointers and synchronise before
+ *    returning.  `_dev` entry points take DEVICE pointers and a cudaStream_t
+ *    (passed as void*; NULL is the CUDA default stream, as in any CUDA API) and
+ *    are asynchronous with respect to the host, except where a result is returned
+ *    in host memory (roots), which synchronises that stream.
+ *  - All entry points are thread-safe.
+ */
+#ifndef ZKB200_H
+#define ZKB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ZKB_API __attribute__((visibility("default")))
+#else
+#define ZKB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZKB_OK 0
+#define ZKB_DECLINED 1
+#define ZKB_ERR_INVALID (-1)
+#define ZKB_ERR_CUDA (-2)
+#define ZKB_ERR_OOM (-3)
+#define ZKB_ERR_UNSUPPORTED (-4)
+#define ZKB_ERR_INTERNAL (-5)
+#define ZKB_ERR_TIMEOUT (-6)
+
+#define ZKB_FIELD_BABYBEAR 0
+#define ZKB_FIELD_GOLDILOCKS 1
+
+/* ------------------------------------------------------------------ general */
+/* Library version string. */
+ZKB_API const char *zkb_version(void);
+/* Thread-local message of the last failed call (zkf-ffi zkf_last_error_message,
+ * zkf-ffi/src/lib.rs:165-171). */
+ZKB_API const char *zkb_last_error_message(void);
+/* Number of CUDA devices; 0 when no usable device (MetalContext availability,
+ * zkf-metal/src/device.rs:1469-1493). */
+ZKB_API int zkb_device_count(void);
+/* Select the device used by this thread's subsequent calls. */
+ZKB_API int zkb_set_device(int device);
+
+/* ---------------------------------------------------------------- Poseidon2 */
+/* flatten_round_constants(seed) (zkf-metal/src/poseidon2/babybear.rs:76-111,
+ * goldilocks.rs:42-83).  Writes up to `cap` canonical constants in the layout
+ * [external initial | internal | external terminal]; returns the count (>0) or <0. */
+ZKB_API int zkb_poseidon2_babybear_round_constants(uint64_t seed, uint32_t *out, size_t cap,
+                                           uint32_t *n_external_rounds,
+                                           uint32_t *n_internal_rounds);
+ZKB_API int zkb_poseidon2_goldilocks_round_constants(uint64_t seed, uint32_t width, uint64_t *out,
+                                             size_t cap, uint32_t *n_external_rounds,
+                                             uint32_t *n_internal_rounds);
+
+/* Poseidon2Accelerator::batch_permute_babybear (zkf-core/src/acceleration.rs:113-145;
+ * MetalPoseidon2::batch_permute_babybear, zkf-metal/src/poseidon2/mod.rs:150-257).
+ * In-place width-16 permutations of n_elems/16 states. */
+ZKB_API int zkb_poseidon2_babybear_permute(uint32_t *states, size_t n_elems, const uint32_t *round_constants,
+                                   size_t n_rc, uint32_t n_external_rounds,
+                                   uint32_t n_internal_rounds);
+/* Poseidon2Accelerator::batch_permute_goldilocks (acceleration.rs:113-145;
+ * MetalPoseidon2::batch_permute_goldilocks, poseidon2/mod.rs:36-148).  Width 16. */
+ZKB_API int zkb_poseidon2_goldilocks_permute(uint64_t *states, size_t n_elems,
+                                     const uint64_t *round_constants, size_t n_rc,
+                                     uint32_t n_external_rounds, uint32_t n_internal_rounds);
+/* Device-pointer forms of the two permutations above. */
+ZKB_API int zkb_poseidon2_babybear_permute_dev(uint32_t *d_states, size_t n_elems,
+                                       const uint32_t *round_constants, size_t n_rc,
+                                       uint32_t n_external_rounds, uint32_t n_internal_rounds,
+                                       void *stream);
+ZKB_API int zkb_poseidon2_goldilocks_permute_dev(uint64_t *d_states, size_t n_elems,
+                                         const uint64_t *round_constants, size_t n_rc,
+                                         uint32_t n_external_rounds, uint32_t n_internal_rounds,
+                                         void *stream);
+
+/* ---------------------------------------------------------------------- DFT */
+/* TwoAdicSubgroupDft::dft_batch / MetalDft::idft_batch
+ * (zkf-metal/src/ntt/p3_adapter.rs:69-106,426-459): column-wise DFT of a row-major
+ * 2^log_h x width matrix, natural order in and out, in place.  inverse=1 applies
+ * g^-1 twiddles and the 1/n scale. */
+ZKB_API int zkb_dft_batch(int field, void *rowmajor, uint32_t log_h, uint32_t width, int inverse);
+ZKB_API int zkb_dft_batch_dev(int field, void *d_rowmajor, uint32_t log_h, uint32_t width, int inverse,
+                      void *stream);
+
+/* p3 coset_lde_batch(trace, log_blowup, shift) followed, when bitrev_rows=1, by
+ * bit_reverse_rows — the LDE that TwoAdicFriPcs::commit hands to the MMCS
+ * (zkf-backends/src/plonky3.rs:250-262 -> p3-dft 0.4.2;
+ * zkf-backends/src/wrapping/stark_to_groth16.rs:2324-2346).  `out` holds
+ * 2^(log_h+log_blowup) x width elements.  shift = 0 selects the field generator. */
+ZKB_API int zkb_coset_lde_batch(int field, const void *trace, uint32_t log_h, uint32_t width,
+                        uint32_t log_blowup, uint64_t shift, int bitrev_rows, void *out);
+ZKB_API int zkb_coset_lde_batch_dev(int field, const void *d_trace, uint32_t log_h, uint32_t width,
+                            uint32_t log_blowup, uint64_t shift, int bitrev_rows, void *d_out,
+                            void *stream);
+
+/* ------------------------------------------------------------------- MMCS */
+/* A row-major matrix: `data` is a host or device pointer depending on the call. */
+typedef struct {
+  const void *data;
+  uint64_t height;
+  uint64_t width;
+} zkb_matrix;
+
+/* Poseidon2 hash configuration of an MMCS: PaddingFreeSponge<Perm, W, 8, OUT> leaves
+ * and TruncatedPermutation<Perm, 2, OUT, W> nodes (zkf-backends/src/plonky3.rs:55-56),
+ * Perm = Poseidon2 of `width` (16; Goldilocks also 12 with OUT = 4) with the
+ * constants of `seed` (plonky3.rs:614-620, 1104-1111). */
+typedef struct {
+  int field;
+  uint32_t width;
+  uint64_t seed;
+} zkb_hasher;
+
+typedef struct zkb_tree zkb_tree;
+
+/* Mmcs::commit (MetalMerkleTreeMmcs::commit, zkf-metal/src/merkle.rs:76-105;
+ * p3 MerkleTree::new, vendor/p3-merkle-tree-gpu/src/merkle_tree.rs:84-151), with no
+ * width limit.  Matrices of several heights are allowed under p3's rule (heights
+ * that round up to the same power of two are equal).  Host form: matrices are host
+ * pointers and are copied to the device.  `root_out` receives OUT elements.
+ * `tree_out` (may be NULL) receives the prover data, freed with zkb_tree_free. */
+ZKB_API int zkb_mmcs_commit(const zkb_hasher *hasher, const zkb_matrix *mats, size_t n_mats,
+                    void *root_out, zkb_tree **tree_out);
+/* Device form: matrices are device pointers that must outlive the tree. */
+ZKB_API int zkb_mmcs_commit_dev(const zkb_hasher *hasher, const zkb_matrix *d_mats, size_t n_mats,
+                        void *root_out, zkb_tree **tree_out, void *stream);
+/* Digest layers (MerkleTree::digest_layers, merkle_tree.rs:40-54). */
+ZKB_API int zkb_tree_num_layers(const zkb_tree *tree);
+ZKB_API int64_t zkb_tree_layer_len(const zkb_tree *tree, int layer);
+ZKB_API int zkb_tree_digest_elems(const zkb_tree *tree);
+ZKB_API int zkb_tree_copy_layer(const zkb_tree *tree, int layer, void *host_out);
+/* Mmcs::open_batch (vendor/p3-merkle-tree-gpu/src/mmcs.rs:179-210): rows of every
+ * committed matrix at the reduced index, concatenated in commit order, and the
+ * log2(max_height) sibling digests. */
+ZKB_API int zkb_mmcs_open_batch(const zkb_tree *tree, uint64_t index, void *rows_out, size_t rows_cap,
+                        void *siblings_out, size_t siblings_cap);
+ZKB_API void zkb_tree_free(zkb_tree *tree);
+
+/* ---------------------------------------------------------------------- FRI */
+/* FriAccelerator::fold_goldilocks (zkf-core/src/acceleration.rs:197-217) and
+ * MetalFri::fold_{goldilocks,babybear} (zkf-metal/src/fri.rs:36-147):
+ *   out[i] = (e[2i] + e[2i+1]) / 2 + alpha * (e[2i] - e[2i+1]) * inv_twiddles[i].
+ * n_evals is even; out holds n_evals/2 elements.  inv_twiddles = NULL selects
+ * g^-rev(i)/2 with g = two_adic_generator(log2(n_evals)), which makes the fold
+ * equal to p3 TwoAdicFriFolding::fold_matrix. */
+ZKB_API int zkb_fri_fold_goldilocks(const uint64_t *evals, size_t n_evals, uint64_t alpha,
+                            const uint64_t *inv_twiddles, uint64_t *out);
+ZKB_API int zkb_fri_fold_babybear(const uint32_t *evals, size_t n_evals, uint32_t alpha,
+                          const uint32_t *inv_twiddles, uint32_t *out);
+/* p3 TwoAdicFriFolding::fold_matrix over the BabyBear quartic extension
+ * (BinomialExtensionField<BabyBear, 4>, x^4 = 11): evals holds 2*n_out extension
+ * elements (4 u32 each) in bit-reversed domain order; beta is 4 u32. */
+ZKB_API int zkb_fri_fold_babybear_ext4(const uint32_t *evals, size_t n_out, const uint32_t *beta,
+                               uint32_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZKB200_H */

@@ -1,0 +1,72 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol that
+include/zkb200.h declares, and its host-side logic (Poseidon2 constant
+generation, argument validation, the no-device decline) behaves."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import ziros_b200 as Z
+from ziros_b200 import _native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "zkb200.h")).read()
+    return sorted(set(re.findall(r"ZKB_API[^;(]*?\b(zkb_\w+)\s*\(", text)))
+
+
+def test_header_declares_exported_symbols():
+    syms = header_symbols()
+    assert len(syms) >= 20
+    lib = N.load()
+    for s in syms:
+        assert hasattr(lib, s), s
+    # the ctypes table covers exactly the header
+    assert sorted(N.SIGNATURES) == syms
+
+
+def test_exported_symbols_in_dynamic_table():
+    import subprocess
+
+    out = subprocess.run(["nm", "-D", "--defined-only", N.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (zkb_\w+)", out))
+    assert set(header_symbols()) <= exported
+
+
+@pytest.mark.parametrize("field,width", [(Z.BABYBEAR, 16), (Z.GOLDILOCKS, 16), (Z.GOLDILOCKS, 12)])
+@pytest.mark.parametrize("seed", [0, 42, 0xDEADBEEFCAFEF00D])
+def test_round_constants_match_oracle(oracle, field, width, seed):
+    ours, ne, ni = Z.round_constants(field, seed, width)
+    ref, rf, rp = oracle.round_constants(field, seed, width)
+    assert (ne, ni) == (rf, rp)
+    assert (ours == ref).all()
+
+
+def test_round_constants_capacity_error():
+    lib = N.load()
+    import ctypes as C
+
+    buf = np.zeros(4, np.uint32)
+    rc = lib.zkb_poseidon2_babybear_round_constants(1, buf.ctypes.data_as(C.c_void_p), 4, None, None)
+    assert rc == N.ERR_INVALID
+    assert "capacity" in N.last_error()
+
+
+def test_version_and_errors_are_strings():
+    assert N.load().zkb_version().startswith(b"zkb200")
+    assert isinstance(N.last_error(), str)
+
+
+@pytest.mark.skipif(N.device_count() > 0, reason="exercises the no-device decline path")
+def test_no_device_declines():
+    assert Z.CudaPoseidon2.new() is None
+    assert Z.CudaFri.new() is None
+    p = Z.CudaPoseidon2()
+    rc, ne, ni = Z.round_constants(Z.BABYBEAR, 1)
+    assert p.batch_permute_babybear(np.zeros(16, np.uint32), rc, ne, ni) is False
+    assert "no CUDA device" in N.last_error()
+    with pytest.raises(N.ZkbDeclined):
+        Z.CudaDft(Z.GOLDILOCKS).dft_batch(np.arange(8, dtype=np.uint64))

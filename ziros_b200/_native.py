@@ -1,0 +1,122 @@
+"""ctypes binding of libzkb200.so (the C ABI declared in include/zkb200.h).
+
+The shared library is built in-tree (``ziros_b200/libzkb200.so``).  Importing
+this module never falls back to anything: a missing or unloadable library raises
+``ZkbError`` so a GPU run can not silently take another path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libzkb200.so")
+
+OK = 0
+DECLINED = 1
+ERR_INVALID = -1
+ERR_CUDA = -2
+ERR_OOM = -3
+ERR_UNSUPPORTED = -4
+ERR_INTERNAL = -5
+ERR_TIMEOUT = -6
+
+FIELD_BABYBEAR = 0
+FIELD_GOLDILOCKS = 1
+
+
+class ZkbError(RuntimeError):
+    """A failed library call; `code` is the C status, the message is zkb_last_error_message()."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"zkb200 error {code}: {message}")
+        self.code = code
+
+
+class ZkbDeclined(ZkbError):
+    """The library declined the call (reference `false`/`None`: use the CPU path)."""
+
+
+class Matrix(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("height", C.c_uint64), ("width", C.c_uint64)]
+
+
+class Hasher(C.Structure):
+    _fields_ = [("field", C.c_int), ("width", C.c_uint32), ("seed", C.c_uint64)]
+
+
+# Every symbol of include/zkb200.h with its ctypes signature.
+_P = C.c_void_p
+_SZ = C.c_size_t
+_U32 = C.c_uint32
+_U64 = C.c_uint64
+_I = C.c_int
+SIGNATURES = {
+    "zkb_version": (C.c_char_p, []),
+    "zkb_last_error_message": (C.c_char_p, []),
+    "zkb_device_count": (_I, []),
+    "zkb_set_device": (_I, [_I]),
+    "zkb_poseidon2_babybear_round_constants": (_I, [_U64, _P, _SZ, _P, _P]),
+    "zkb_poseidon2_goldilocks_round_constants": (_I, [_U64, _U32, _P, _SZ, _P, _P]),
+    "zkb_poseidon2_babybear_permute": (_I, [_P, _SZ, _P, _SZ, _U32, _U32]),
+    "zkb_poseidon2_goldilocks_permute": (_I, [_P, _SZ, _P, _SZ, _U32, _U32]),
+    "zkb_poseidon2_babybear_permute_dev": (_I, [_P, _SZ, _P, _SZ, _U32, _U32, _P]),
+    "zkb_poseidon2_goldilocks_permute_dev": (_I, [_P, _SZ, _P, _SZ, _U32, _U32, _P]),
+    "zkb_dft_batch": (_I, [_I, _P, _U32, _U32, _I]),
+    "zkb_dft_batch_dev": (_I, [_I, _P, _U32, _U32, _I, _P]),
+    "zkb_coset_lde_batch": (_I, [_I, _P, _U32, _U32, _U32, _U64, _I, _P]),
+    "zkb_coset_lde_batch_dev": (_I, [_I, _P, _U32, _U32, _U32, _U64, _I, _P, _P]),
+    "zkb_mmcs_commit": (_I, [_P, _P, _SZ, _P, _P]),
+    "zkb_mmcs_commit_dev": (_I, [_P, _P, _SZ, _P, _P, _P]),
+    "zkb_tree_num_layers": (_I, [_P]),
+    "zkb_tree_layer_len": (C.c_int64, [_P, _I]),
+    "zkb_tree_digest_elems": (_I, [_P]),
+    "zkb_tree_copy_layer": (_I, [_P, _I, _P]),
+    "zkb_mmcs_open_batch": (_I, [_P, _U64, _P, _SZ, _P, _SZ]),
+    "zkb_tree_free": (None, [_P]),
+    "zkb_fri_fold_goldilocks": (_I, [_P, _SZ, _U64, _P, _P]),
+    "zkb_fri_fold_babybear": (_I, [_P, _SZ, _U32, _P, _P]),
+    "zkb_fri_fold_babybear_ext4": (_I, [_P, _SZ, _P, _P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load libzkb200.so (raises ZkbError if it is missing or incomplete)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ZkbError(ERR_INTERNAL, f"{LIB_PATH} is not built (run ziros_b200.build.build())")
+        try:
+            lib = C.CDLL(LIB_PATH)
+        except OSError as e:  # pragma: no cover - depends on the environment
+            raise ZkbError(ERR_INTERNAL, f"cannot load {LIB_PATH}: {e}") from e
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error() -> str:
+    msg = load().zkb_last_error_message()
+    return msg.decode() if msg else ""
+
+
+def check(rc: int) -> int:
+    """Raise on a negative status; DECLINED raises ZkbDeclined."""
+    if rc == OK or rc > DECLINED:
+        return rc
+    if rc == DECLINED:
+        raise ZkbDeclined(rc, last_error())
+    raise ZkbError(rc, last_error())
+
+
+def device_count() -> int:
+    return int(load().zkb_device_count())

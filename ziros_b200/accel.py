@@ -1,0 +1,286 @@
+"""Host-side mirror of the reference's accelerator types over the C ABI.
+
+Each class keeps the name, argument meaning and error behaviour of the ZirOS
+type it stands in for (paths relative to the ZirOS repository root):
+
+  CudaPoseidon2        <- MetalPoseidon2          zkf-metal/src/poseidon2/mod.rs:21-257
+  CudaDft              <- MetalDft<F>             zkf-metal/src/ntt/p3_adapter.rs:36-459
+  CudaMerkleTreeMmcs   <- MetalMerkleTreeMmcs     zkf-metal/src/merkle.rs:33-138
+  CudaFri              <- MetalFri                zkf-metal/src/fri.rs:18-147
+
+``new()`` returns None when no CUDA device is present, as ``MetalX::new()`` does
+without a Metal device; batch calls return ``False`` / ``None`` when the library
+declines (the caller then takes its CPU path).  Any other failure raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+
+BABYBEAR = N.FIELD_BABYBEAR
+GOLDILOCKS = N.FIELD_GOLDILOCKS
+BB_P = 0x78000001
+GL_P = 0xFFFFFFFF00000001
+
+
+def dtype_of(field: int):
+    return np.uint32 if field == BABYBEAR else np.uint64
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _torch_ptr_stream(t):
+    import torch
+
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    return C.c_void_p(t.data_ptr()), C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def round_constants(field: int, seed: int, width: int = 16) -> Tuple[np.ndarray, int, int]:
+    """flatten_round_constants(seed) (zkf-metal/src/poseidon2/{babybear,goldilocks}.rs)."""
+    lib = N.load()
+    out = np.zeros(512, dtype=dtype_of(field))
+    ne, ni = C.c_uint32(), C.c_uint32()
+    if field == BABYBEAR:
+        if width != 16:
+            raise ValueError("BabyBear Poseidon2 is width 16")
+        n = lib.zkb_poseidon2_babybear_round_constants(seed, _ptr(out), out.size, C.byref(ne), C.byref(ni))
+    else:
+        n = lib.zkb_poseidon2_goldilocks_round_constants(seed, width, _ptr(out), out.size, C.byref(ne),
+                                                         C.byref(ni))
+    N.check(n)
+    return out[:n].copy(), ne.value, ni.value
+
+
+def _have_device() -> bool:
+    return N.device_count() > 0
+
+
+# --------------------------------------------------------------------- Poseidon2
+class CudaPoseidon2:
+    """Batch Poseidon2 width-16 permutations (MetalPoseidon2)."""
+
+    @staticmethod
+    def new() -> Optional["CudaPoseidon2"]:
+        N.load()
+        return CudaPoseidon2() if _have_device() else None
+
+    def batch_permute_babybear(self, states: np.ndarray, round_constants: np.ndarray,
+                               n_external_rounds: int, n_internal_rounds: int) -> bool:
+        """In-place; False when declined (poseidon2/mod.rs:150-257)."""
+        return self._permute(BABYBEAR, states, round_constants, n_external_rounds, n_internal_rounds)
+
+    def batch_permute_goldilocks(self, states: np.ndarray, round_constants: np.ndarray,
+                                 n_external_rounds: int, n_internal_rounds: int) -> bool:
+        """In-place; False when declined (poseidon2/mod.rs:36-148)."""
+        return self._permute(GOLDILOCKS, states, round_constants, n_external_rounds, n_internal_rounds)
+
+    def _permute(self, field, states, rc, ne, ni) -> bool:
+        dt = dtype_of(field)
+        if states.dtype != dt or not states.flags.c_contiguous:
+            raise TypeError(f"states must be a contiguous {np.dtype(dt).name} array")
+        rc = np.ascontiguousarray(rc, dtype=dt)
+        lib = N.load()
+        fn = lib.zkb_poseidon2_babybear_permute if field == BABYBEAR else lib.zkb_poseidon2_goldilocks_permute
+        try:
+            N.check(fn(_ptr(states), states.size, _ptr(rc), rc.size, ne, ni))
+        except N.ZkbDeclined:
+            return False
+        return True
+
+    def batch_permute_dev(self, field: int, states, round_constants: np.ndarray,
+                          n_external_rounds: int, n_internal_rounds: int) -> None:
+        """Device-resident form on a CUDA torch tensor, on the tensor's current stream."""
+        rc = np.ascontiguousarray(round_constants, dtype=dtype_of(field))
+        ptr, stream = _torch_ptr_stream(states)
+        lib = N.load()
+        fn = (lib.zkb_poseidon2_babybear_permute_dev if field == BABYBEAR
+              else lib.zkb_poseidon2_goldilocks_permute_dev)
+        N.check(fn(ptr, states.numel(), _ptr(rc), rc.size, n_external_rounds, n_internal_rounds, stream))
+
+
+# --------------------------------------------------------------------------- DFT
+class CudaDft:
+    """TwoAdicSubgroupDft over a row-major matrix (MetalDft<F>)."""
+
+    def __init__(self, field: int):
+        N.load()
+        self.field = field
+
+    @staticmethod
+    def new(field: int) -> Optional["CudaDft"]:
+        N.load()
+        return CudaDft(field) if _have_device() else None
+
+    def _mat(self, mat: np.ndarray) -> np.ndarray:
+        m = np.ascontiguousarray(mat, dtype=dtype_of(self.field))
+        if m.ndim == 1:
+            m = m.reshape(-1, 1)
+        h = m.shape[0]
+        if h == 0 or h & (h - 1):
+            raise ValueError("height must be a power of two")
+        return m
+
+    def dft_batch(self, mat: np.ndarray) -> np.ndarray:
+        m = self._mat(mat).copy()
+        N.check(N.load().zkb_dft_batch(self.field, _ptr(m), m.shape[0].bit_length() - 1, m.shape[1], 0))
+        return m
+
+    def idft_batch(self, mat: np.ndarray) -> np.ndarray:
+        m = self._mat(mat).copy()
+        N.check(N.load().zkb_dft_batch(self.field, _ptr(m), m.shape[0].bit_length() - 1, m.shape[1], 1))
+        return m
+
+    def coset_lde_batch(self, mat: np.ndarray, added_bits: int, shift: Optional[int] = None,
+                        bit_reverse_rows: bool = False) -> np.ndarray:
+        """p3 coset_lde_batch (natural order), or the PCS's bit-reversed rows."""
+        m = self._mat(mat)
+        out = np.zeros((m.shape[0] << added_bits, m.shape[1]), dtype=dtype_of(self.field))
+        N.check(N.load().zkb_coset_lde_batch(self.field, _ptr(m), m.shape[0].bit_length() - 1, m.shape[1],
+                                             added_bits, shift or 0, int(bit_reverse_rows), _ptr(out)))
+        return out
+
+    def coset_lde_batch_dev(self, trace, log_blowup: int, out, shift: Optional[int] = None,
+                            bit_reverse_rows: bool = True) -> None:
+        """Device form on CUDA torch tensors (trace: h x w, out: (h << log_blowup) x w)."""
+        h, w = trace.shape
+        tp, stream = _torch_ptr_stream(trace)
+        op, _ = _torch_ptr_stream(out)
+        if out.shape[0] != h << log_blowup or out.shape[1] != w:
+            raise ValueError("output shape mismatch")
+        N.check(N.load().zkb_coset_lde_batch_dev(self.field, tp, h.bit_length() - 1, w, log_blowup,
+                                                 shift or 0, int(bit_reverse_rows), op, stream))
+
+
+# -------------------------------------------------------------------------- MMCS
+class Tree:
+    """Prover data of a commitment (p3 MerkleTree): digest layers stay on the device."""
+
+    def __init__(self, handle: C.c_void_p, field: int, mats: Sequence[np.ndarray]):
+        self._h = handle
+        self.field = field
+        self.widths = [m.shape[1] for m in mats]
+        self.heights = [m.shape[0] for m in mats]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.load().zkb_tree_free(h)
+            self._h = None
+
+    @property
+    def digest_elems(self) -> int:
+        return N.load().zkb_tree_digest_elems(self._h)
+
+    def num_layers(self) -> int:
+        return N.load().zkb_tree_num_layers(self._h)
+
+    def layer(self, i: int) -> np.ndarray:
+        lib = N.load()
+        n = lib.zkb_tree_layer_len(self._h, i)
+        N.check(n if n < 0 else 0)
+        out = np.zeros((n, self.digest_elems), dtype=dtype_of(self.field))
+        N.check(lib.zkb_tree_copy_layer(self._h, i, _ptr(out)))
+        return out
+
+    def digest_layers(self) -> List[np.ndarray]:
+        return [self.layer(i) for i in range(self.num_layers())]
+
+    def root(self) -> np.ndarray:
+        return self.layer(self.num_layers() - 1)[0]
+
+
+class CudaMerkleTreeMmcs:
+    """Poseidon2 MMCS (MetalMerkleTreeMmcs / p3 MerkleTreeMmcs) with device-resident layers."""
+
+    def __init__(self, field: int, seed: int, width: int = 16):
+        N.load()
+        self.field = field
+        self.hasher = N.Hasher(field, width, seed)
+        self.digest_elems = 8 if width == 16 else 4
+
+    def commit(self, mats: Sequence[np.ndarray]) -> Tuple[np.ndarray, Tree]:
+        """Mmcs::commit -> (root, prover data)."""
+        dt = dtype_of(self.field)
+        mats = [np.ascontiguousarray(m, dtype=dt) for m in mats]
+        descs = (N.Matrix * len(mats))(*[N.Matrix(m.ctypes.data, m.shape[0], m.shape[1]) for m in mats])
+        root = np.zeros(self.digest_elems, dtype=dt)
+        handle = C.c_void_p()
+        N.check(N.load().zkb_mmcs_commit(C.byref(self.hasher), descs, len(mats), _ptr(root), C.byref(handle)))
+        return root, Tree(handle, self.field, mats)
+
+    def commit_dev(self, mats) -> Tuple[np.ndarray, Tree]:
+        """Commit CUDA torch tensors in place; they must outlive the returned tree."""
+        import torch
+
+        descs = (N.Matrix * len(mats))(*[N.Matrix(m.data_ptr(), m.shape[0], m.shape[1]) for m in mats])
+        root = np.zeros(self.digest_elems, dtype=dtype_of(self.field))
+        handle = C.c_void_p()
+        stream = C.c_void_p(torch.cuda.current_stream(mats[0].device).cuda_stream)
+        N.check(N.load().zkb_mmcs_commit_dev(C.byref(self.hasher), descs, len(mats), _ptr(root),
+                                             C.byref(handle), stream))
+        t = Tree(handle, self.field, [np.empty((m.shape[0], m.shape[1]), dtype=np.uint8) for m in mats])
+        t._keepalive = list(mats)
+        return root, t
+
+    def open_batch(self, index: int, tree: Tree) -> Tuple[List[np.ndarray], List[np.ndarray]]:
+        """Mmcs::open_batch -> (rows per matrix, sibling digests)."""
+        dt = dtype_of(self.field)
+        total_w = sum(tree.widths)
+        log_max = (max(tree.heights) - 1).bit_length()
+        rows = np.zeros(max(total_w, 1), dtype=dt)
+        sib = np.zeros(max(log_max * self.digest_elems, 1), dtype=dt)
+        N.check(N.load().zkb_mmcs_open_batch(tree._h, index, _ptr(rows), rows.size, _ptr(sib), sib.size))
+        out, off = [], 0
+        for w in tree.widths:
+            out.append(rows[off:off + w].copy())
+            off += w
+        return out, [sib[i * self.digest_elems:(i + 1) * self.digest_elems].copy() for i in range(log_max)]
+
+
+# --------------------------------------------------------------------------- FRI
+class CudaFri:
+    """FRI folding (MetalFri / FriAccelerator)."""
+
+    @staticmethod
+    def new() -> Optional["CudaFri"]:
+        N.load()
+        return CudaFri() if _have_device() else None
+
+    def _fold(self, field, evals, alpha, inv_twiddles):
+        dt = dtype_of(field)
+        e = np.ascontiguousarray(evals, dtype=dt)
+        if e.size % 2:
+            return None
+        t = None if inv_twiddles is None else np.ascontiguousarray(inv_twiddles, dtype=dt)
+        if t is not None and t.size != e.size // 2:
+            return None
+        out = np.zeros(e.size // 2, dtype=dt)
+        lib = N.load()
+        fn = lib.zkb_fri_fold_goldilocks if field == GOLDILOCKS else lib.zkb_fri_fold_babybear
+        try:
+            N.check(fn(_ptr(e), e.size, alpha, None if t is None else _ptr(t), _ptr(out)))
+        except N.ZkbDeclined:
+            return None
+        return out
+
+    def fold_goldilocks(self, evals, alpha: int, inv_twiddles=None) -> Optional[np.ndarray]:
+        return self._fold(GOLDILOCKS, evals, alpha, inv_twiddles)
+
+    def fold_babybear(self, evals, alpha: int, inv_twiddles=None) -> Optional[np.ndarray]:
+        return self._fold(BABYBEAR, evals, alpha, inv_twiddles)
+
+    def fold_babybear_ext4(self, evals: np.ndarray, beta) -> np.ndarray:
+        """p3 fold_matrix over BabyBear^4; evals: (2n, 4) u32 -> (n, 4)."""
+        e = np.ascontiguousarray(evals, dtype=np.uint32).reshape(-1, 4)
+        b = np.ascontiguousarray(beta, dtype=np.uint32)
+        out = np.zeros((e.shape[0] // 2, 4), dtype=np.uint32)
+        N.check(N.load().zkb_fri_fold_babybear_ext4(_ptr(e), out.shape[0], _ptr(b), _ptr(out)))
+        return out

@@ -1,0 +1,387 @@
+// abi.cu — extern "C" entry points declared in include/zkb200.h.
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.cuh"
+
+namespace zkb {
+const char *last_error();
+}
+
+using namespace zkb;
+
+struct zkb_tree {
+  DeviceTree t;
+};
+
+namespace {
+
+// Declines (reference fallback semantics) when the process has no usable device.
+int require_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_error("no CUDA device available (%s)", e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+    return ZKB_DECLINED;
+  }
+  return ZKB_OK;
+}
+
+#define ZKB_ENTRY() \
+  clear_error();    \
+  ZKB_TRY(require_device())
+
+// Host buffer <-> device scratch helpers for the host-pointer entry points.
+int to_device(ScratchBuf &buf, const void *host, size_t bytes, cudaStream_t s) {
+  ZKB_TRY(buf.alloc(bytes, s));
+  if (bytes) ZKB_CHECK_CUDA(cudaMemcpyAsync(buf.p, host, bytes, cudaMemcpyHostToDevice, s));
+  return ZKB_OK;
+}
+
+int to_host(void *host, const void *dev, size_t bytes, cudaStream_t s) {
+  if (bytes) ZKB_CHECK_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s));
+  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  return ZKB_OK;
+}
+
+template <class F>
+int permute_dev_impl(typename F::T *d_states, size_t n_elems, const typename F::T *rc, size_t n_rc,
+                     uint32_t n_ext, uint32_t n_int, cudaStream_t s) {
+  ZKB_REQUIRE(n_elems % 16 == 0, "state buffer length %zu is not a multiple of 16", n_elems);
+  ZKB_REQUIRE(rc != nullptr || n_rc == 0, "null round constants");
+  const int field = sizeof(typename F::T) == 4 ? FIELD_BABYBEAR : FIELD_GOLDILOCKS;
+  std::vector<uint64_t> rc64(rc, rc + n_rc);
+  std::vector<uint64_t> diag = p2_diagonal(field, 16);
+  P2Params<F, 16> p;
+  if (!build_p2_params<F, 16>(rc64.data(), n_rc, (int)n_ext, (int)n_int, diag.data(), 8, &p)) {
+    set_error("round constants do not match n_external_rounds=%u n_internal_rounds=%u (n_rc=%zu)",
+              n_ext, n_int, n_rc);
+    return ZKB_ERR_INVALID;
+  }
+  return p2_permute_batch<F, 16>(d_states, n_elems / 16, p, s);
+}
+
+template <class F>
+int permute_host_impl(typename F::T *states, size_t n_elems, const typename F::T *rc, size_t n_rc,
+                      uint32_t n_ext, uint32_t n_int) {
+  using T = typename F::T;
+  ZKB_REQUIRE(states != nullptr || n_elems == 0, "null states");
+  cudaStream_t s = thread_stream();
+  ScratchBuf d;
+  ZKB_TRY(to_device(d, states, n_elems * sizeof(T), s));
+  ZKB_TRY(permute_dev_impl<F>(d.as<T>(), n_elems, rc, n_rc, n_ext, n_int, s));
+  return to_host(states, d.p, n_elems * sizeof(T), s);
+}
+
+int check_field(int field) {
+  ZKB_REQUIRE(field == ZKB_FIELD_BABYBEAR || field == ZKB_FIELD_GOLDILOCKS, "unknown field %d", field);
+  return ZKB_OK;
+}
+
+int hasher_spec(const zkb_hasher *h, HasherSpec *spec) {
+  ZKB_REQUIRE(h != nullptr, "null hasher");
+  ZKB_TRY(check_field(h->field));
+  if (!make_hasher_spec(h->field, (int)h->width, h->seed, spec)) {
+    set_error("unsupported Poseidon2 hasher: field %d width %u", h->field, h->width);
+    return ZKB_ERR_UNSUPPORTED;
+  }
+  return ZKB_OK;
+}
+
+int tree_from(zkb_tree **tree_out, std::unique_ptr<zkb_tree> &tree, void *root_out, cudaStream_t s) {
+  if (root_out) ZKB_TRY(mmcs_root_to_host(&tree->t, root_out, s));
+  if (tree_out)
+    *tree_out = tree.release();
+  else
+    ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  return ZKB_OK;
+}
+
+template <class F>
+int fold_host(const typename F::T *evals, size_t n_evals, typename F::T alpha,
+                     const typename F::T *inv_tw, typename F::T *out) {
+  using T = typename F::T;
+  ZKB_REQUIRE(n_evals % 2 == 0, "odd number of evaluations");
+  ZKB_REQUIRE((evals && out) || n_evals == 0, "null buffers");
+  const size_t n_out = n_evals / 2;
+  cudaStream_t s = thread_stream();
+  ScratchBuf de, dt, dout;
+  ZKB_TRY(to_device(de, evals, n_evals * sizeof(T), s));
+  if (inv_tw) ZKB_TRY(to_device(dt, inv_tw, n_out * sizeof(T), s));
+  ZKB_TRY(dout.alloc(n_out * sizeof(T), s));
+  ZKB_TRY(fri_fold_base_dev<F>(de.as<T>(), n_out, alpha, inv_tw ? dt.as<T>() : nullptr, dout.as<T>(), s));
+  return to_host(out, dout.p, n_out * sizeof(T), s);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *zkb_version(void) { return "zkb200 0.1.0 (sm_100a)"; }
+
+const char *zkb_last_error_message(void) { return last_error(); }
+
+int zkb_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int zkb_set_device(int device) {
+  clear_error();
+  ZKB_CHECK_CUDA(cudaSetDevice(device));
+  return ZKB_OK;
+}
+
+// ------------------------------------------------------------------ Poseidon2
+int zkb_poseidon2_babybear_round_constants(uint64_t seed, uint32_t *out, size_t cap,
+                                           uint32_t *n_ext, uint32_t *n_int) {
+  clear_error();
+  int rf, rp;
+  p2_round_numbers(FIELD_BABYBEAR, 16, &rf, &rp);
+  std::vector<uint64_t> flat = p2_flat_constants(FIELD_BABYBEAR, 16, seed);
+  ZKB_REQUIRE(out != nullptr && cap >= flat.size(), "output capacity %zu < %zu", cap, flat.size());
+  for (size_t i = 0; i < flat.size(); i++) out[i] = (uint32_t)flat[i];
+  if (n_ext) *n_ext = (uint32_t)rf;
+  if (n_int) *n_int = (uint32_t)rp;
+  return (int)flat.size();
+}
+
+int zkb_poseidon2_goldilocks_round_constants(uint64_t seed, uint32_t width, uint64_t *out,
+                                             size_t cap, uint32_t *n_ext, uint32_t *n_int) {
+  clear_error();
+  int rf, rp;
+  ZKB_REQUIRE(p2_round_numbers(FIELD_GOLDILOCKS, (int)width, &rf, &rp), "unsupported width %u", width);
+  std::vector<uint64_t> flat = p2_flat_constants(FIELD_GOLDILOCKS, (int)width, seed);
+  ZKB_REQUIRE(out != nullptr && cap >= flat.size(), "output capacity %zu < %zu", cap, flat.size());
+  std::memcpy(out, flat.data(), flat.size() * 8);
+  if (n_ext) *n_ext = (uint32_t)rf;
+  if (n_int) *n_int = (uint32_t)rp;
+  return (int)flat.size();
+}
+
+int zkb_poseidon2_babybear_permute(uint32_t *states, size_t n_elems, const uint32_t *rc, size_t n_rc,
+                                   uint32_t n_ext, uint32_t n_int) {
+  ZKB_ENTRY();
+  return permute_host_impl<BabyBear>(states, n_elems, rc, n_rc, n_ext, n_int);
+}
+
+int zkb_poseidon2_goldilocks_permute(uint64_t *states, size_t n_elems, const uint64_t *rc,
+                                     size_t n_rc, uint32_t n_ext, uint32_t n_int) {
+  ZKB_ENTRY();
+  return permute_host_impl<Goldilocks>(states, n_elems, rc, n_rc, n_ext, n_int);
+}
+
+int zkb_poseidon2_babybear_permute_dev(uint32_t *d_states, size_t n_elems, const uint32_t *rc,
+                                       size_t n_rc, uint32_t n_ext, uint32_t n_int, void *stream) {
+  ZKB_ENTRY();
+  return permute_dev_impl<BabyBear>(d_states, n_elems, rc, n_rc, n_ext, n_int, resolve_stream(stream));
+}
+
+int zkb_poseidon2_goldilocks_permute_dev(uint64_t *d_states, size_t n_elems, const uint64_t *rc,
+                                         size_t n_rc, uint32_t n_ext, uint32_t n_int,
+                                         void *stream) {
+  ZKB_ENTRY();
+  return permute_dev_impl<Goldilocks>(d_states, n_elems, rc, n_rc, n_ext, n_int,
+                                      resolve_stream(stream));
+}
+
+// ------------------------------------------------------------------------ DFT
+int zkb_dft_batch_dev(int field, void *d, uint32_t log_h, uint32_t width, int inverse, void *stream) {
+  ZKB_ENTRY();
+  ZKB_TRY(check_field(field));
+  cudaStream_t s = resolve_stream(stream);
+  if (field == ZKB_FIELD_BABYBEAR)
+    return ntt_dft_dev<BabyBear>((uint32_t *)d, (int)log_h, width, inverse != 0, s);
+  return ntt_dft_dev<Goldilocks>((uint64_t *)d, (int)log_h, width, inverse != 0, s);
+}
+
+int zkb_dft_batch(int field, void *rowmajor, uint32_t log_h, uint32_t width, int inverse) {
+  ZKB_ENTRY();
+  ZKB_TRY(check_field(field));
+  ZKB_REQUIRE(log_h < 40, "log_h too large");
+  const size_t bytes = ((size_t)width << log_h) * field_elem_bytes(field);
+  cudaStream_t s = thread_stream();
+  ScratchBuf d;
+  ZKB_TRY(to_device(d, rowmajor, bytes, s));
+  ZKB_TRY(zkb_dft_batch_dev(field, d.p, log_h, width, inverse, s));
+  return to_host(rowmajor, d.p, bytes, s);
+}
+
+int zkb_coset_lde_batch_dev(int field, const void *d_trace, uint32_t log_h, uint32_t width,
+                            uint32_t log_blowup, uint64_t shift, int bitrev_rows, void *d_out,
+                            void *stream) {
+  ZKB_ENTRY();
+  ZKB_TRY(check_field(field));
+  cudaStream_t s = resolve_stream(stream);
+  if (field == ZKB_FIELD_BABYBEAR) {
+    if (shift == 0) shift = BabyBear::GENERATOR;
+    ZKB_REQUIRE(shift < BabyBear::P, "shift is not canonical");
+    return ntt_lde_dev<BabyBear>((const uint32_t *)d_trace, (int)log_h, width, (int)log_blowup,
+                                 (uint32_t)shift, bitrev_rows != 0, (uint32_t *)d_out, s);
+  }
+  if (shift == 0) shift = Goldilocks::GENERATOR;
+  ZKB_REQUIRE(shift < Goldilocks::P, "shift is not canonical");
+  return ntt_lde_dev<Goldilocks>((const uint64_t *)d_trace, (int)log_h, width, (int)log_blowup, shift,
+                                 bitrev_rows != 0, (uint64_t *)d_out, s);
+}
+
+int zkb_coset_lde_batch(int field, const void *trace, uint32_t log_h, uint32_t width,
+                        uint32_t log_blowup, uint64_t shift, int bitrev_rows, void *out) {
+  ZKB_ENTRY();
+  ZKB_TRY(check_field(field));
+  ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
+  const size_t es = field_elem_bytes(field);
+  const size_t in_bytes = ((size_t)width << log_h) * es;
+  const size_t out_bytes = in_bytes << log_blowup;
+  cudaStream_t s = thread_stream();
+  ScratchBuf din, dout;
+  ZKB_TRY(to_device(din, trace, in_bytes, s));
+  ZKB_TRY(dout.alloc(out_bytes, s));
+  ZKB_TRY(zkb_coset_lde_batch_dev(field, din.p, log_h, width, log_blowup, shift, bitrev_rows, dout.p, s));
+  return to_host(out, dout.p, out_bytes, s);
+}
+
+// ----------------------------------------------------------------------- MMCS
+int zkb_mmcs_commit_dev(const zkb_hasher *hasher, const zkb_matrix *d_mats, size_t n_mats,
+                        void *root_out, zkb_tree **tree_out, void *stream) {
+  ZKB_ENTRY();
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(d_mats != nullptr && n_mats > 0, "No matrices given");
+  cudaStream_t s = resolve_stream(stream);
+  std::vector<TreeMatrix> mats;
+  for (size_t i = 0; i < n_mats; i++) mats.push_back({d_mats[i].data, d_mats[i].height, d_mats[i].width});
+  auto tree = std::make_unique<zkb_tree>();
+  ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));
+  return tree_from(tree_out, tree, root_out, s);
+}
+
+int zkb_mmcs_commit(const zkb_hasher *hasher, const zkb_matrix *mats, size_t n_mats, void *root_out,
+                    zkb_tree **tree_out) {
+  ZKB_ENTRY();
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(mats != nullptr && n_mats > 0, "No matrices given");
+  cudaStream_t s = thread_stream();
+  auto tree = std::make_unique<zkb_tree>();
+  tree->t.stream = s;
+  ZKB_CHECK_CUDA(cudaGetDevice(&tree->t.device));
+  const size_t es = field_elem_bytes(spec.field);
+  std::vector<TreeMatrix> dm;
+  for (size_t i = 0; i < n_mats; i++) {
+    const size_t bytes = mats[i].height * mats[i].width * es;
+    void *p = nullptr;
+    ZKB_TRY(dev_alloc(&p, bytes ? bytes : 16, s));
+    tree->t.owned.push_back(p);
+    if (bytes) ZKB_CHECK_CUDA(cudaMemcpyAsync(p, mats[i].data, bytes, cudaMemcpyHostToDevice, s));
+    dm.push_back({p, mats[i].height, mats[i].width});
+  }
+  ZKB_TRY(mmcs_build_dev(spec, dm, &tree->t, s));
+  return tree_from(tree_out, tree, root_out, s);
+}
+
+int zkb_tree_num_layers(const zkb_tree *tree) {
+  if (!tree) return ZKB_ERR_INVALID;
+  return (int)tree->t.layer_len.size();
+}
+
+int64_t zkb_tree_layer_len(const zkb_tree *tree, int layer) {
+  if (!tree || layer < 0 || layer >= (int)tree->t.layer_len.size()) return ZKB_ERR_INVALID;
+  return (int64_t)tree->t.layer_len[layer];
+}
+
+int zkb_tree_digest_elems(const zkb_tree *tree) {
+  if (!tree) return ZKB_ERR_INVALID;
+  return tree->t.spec.out;
+}
+
+int zkb_tree_copy_layer(const zkb_tree *tree, int layer, void *host_out) {
+  clear_error();
+  ZKB_REQUIRE(tree && layer >= 0 && layer < (int)tree->t.layer_len.size() && host_out,
+              "invalid tree layer request");
+  const DeviceTree &t = tree->t;
+  const size_t es = field_elem_bytes(t.spec.field);
+  const size_t D = t.spec.out;
+  ZKB_CHECK_CUDA(cudaSetDevice(t.device));
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(host_out, (const char *)t.d_layers + t.layer_off[layer] * D * es,
+                                 t.layer_len[layer] * D * es, cudaMemcpyDeviceToHost, t.stream));
+  ZKB_CHECK_CUDA(cudaStreamSynchronize(t.stream));
+  return ZKB_OK;
+}
+
+int zkb_mmcs_open_batch(const zkb_tree *tree, uint64_t index, void *rows_out, size_t rows_cap,
+                        void *siblings_out, size_t siblings_cap) {
+  clear_error();
+  ZKB_REQUIRE(tree != nullptr, "null tree");
+  const DeviceTree &t = tree->t;
+  uint64_t max_h = 0, total_w = 0;
+  for (const TreeMatrix &m : t.mats) {
+    max_h = m.height > max_h ? m.height : max_h;
+    total_w += m.width;
+  }
+  ZKB_REQUIRE(index < max_h, "index %llu out of bounds for height %llu", (unsigned long long)index,
+              (unsigned long long)max_h);
+  int log_max = 0;
+  while ((1ull << log_max) < max_h) log_max++;
+  const size_t es = field_elem_bytes(t.spec.field);
+  const size_t D = t.spec.out;
+  ZKB_REQUIRE(rows_out == nullptr || rows_cap >= total_w, "rows capacity %zu < %llu", rows_cap,
+              (unsigned long long)total_w);
+  ZKB_REQUIRE(siblings_out == nullptr || siblings_cap >= (size_t)log_max * D,
+              "siblings capacity %zu < %zu", siblings_cap, (size_t)log_max * D);
+  ZKB_CHECK_CUDA(cudaSetDevice(t.device));
+  if (rows_out) {
+    size_t off = 0;
+    for (const TreeMatrix &m : t.mats) {
+      int lh = 0;
+      while ((1ull << lh) < m.height) lh++;
+      const uint64_t r = index >> (log_max - lh);
+      ZKB_CHECK_CUDA(cudaMemcpyAsync((char *)rows_out + off * es,
+                                     (const char *)m.data + r * m.width * es, m.width * es,
+                                     cudaMemcpyDeviceToHost, t.stream));
+      off += m.width;
+    }
+  }
+  if (siblings_out) {
+    for (int i = 0; i < log_max; i++) {
+      const uint64_t j = (index >> i) ^ 1ull;
+      ZKB_REQUIRE(j < t.layer_len[i], "sibling outside layer %d", i);
+      ZKB_CHECK_CUDA(cudaMemcpyAsync((char *)siblings_out + (size_t)i * D * es,
+                                     (const char *)t.d_layers + (t.layer_off[i] + j) * D * es, D * es,
+                                     cudaMemcpyDeviceToHost, t.stream));
+    }
+  }
+  ZKB_CHECK_CUDA(cudaStreamSynchronize(t.stream));
+  return ZKB_OK;
+}
+
+void zkb_tree_free(zkb_tree *tree) { delete tree; }
+
+// ------------------------------------------------------------------------ FRI
+int zkb_fri_fold_goldilocks(const uint64_t *evals, size_t n_evals, uint64_t alpha,
+                            const uint64_t *inv_twiddles, uint64_t *out) {
+  ZKB_ENTRY();
+  return fold_host<Goldilocks>(evals, n_evals, alpha, inv_twiddles, out);
+}
+
+int zkb_fri_fold_babybear(const uint32_t *evals, size_t n_evals, uint32_t alpha,
+                          const uint32_t *inv_twiddles, uint32_t *out) {
+  ZKB_ENTRY();
+  return fold_host<BabyBear>(evals, n_evals, alpha, inv_twiddles, out);
+}
+
+int zkb_fri_fold_babybear_ext4(const uint32_t *evals, size_t n_out, const uint32_t *beta, uint32_t *out) {
+  ZKB_ENTRY();
+  ZKB_REQUIRE(beta != nullptr && ((evals && out) || n_out == 0), "null buffers");
+  cudaStream_t s = thread_stream();
+  ScratchBuf de, dout;
+  ZKB_TRY(to_device(de, evals, n_out * 8 * sizeof(uint32_t), s));
+  ZKB_TRY(dout.alloc(n_out * 4 * sizeof(uint32_t), s));
+  ZKB_TRY(fri_fold_ext4_dev(de.as<uint32_t>(), n_out, beta, dout.as<uint32_t>(), s));
+  return to_host(out, dout.p, n_out * 4 * sizeof(uint32_t), s);
+}
+
+}  // extern "C"

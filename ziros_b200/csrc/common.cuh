@@ -1,0 +1,113 @@
+// common.cuh — status codes, last-error convention, device context and memory.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
+#include "../../include/zkb200.h"
+
+namespace zkb {
+
+// Sets the thread-local last-error message (zkf-ffi set_last_error, zkf-ffi/src/lib.rs:49-60).
+void set_error(const char *fmt, ...);
+void clear_error();
+
+#define ZKB_CHECK_CUDA(call)                                                          \
+  do {                                                                                \
+    cudaError_t zkb_e_ = (call);                                                      \
+    if (zkb_e_ != cudaSuccess) {                                                      \
+      ::zkb::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(zkb_e_),     \
+                       __FILE__, __LINE__);                                           \
+      return zkb_e_ == cudaErrorMemoryAllocation ? ZKB_ERR_OOM : ZKB_ERR_CUDA;         \
+    }                                                                                 \
+  } while (0)
+
+#define ZKB_CHECK_LAUNCH() ZKB_CHECK_CUDA(cudaGetLastError())
+
+#define ZKB_TRY(expr)                 \
+  do {                                \
+    int zkb_rc_ = (expr);             \
+    if (zkb_rc_ != ZKB_OK) return zkb_rc_; \
+  } while (0)
+
+#define ZKB_REQUIRE(cond, ...)           \
+  do {                                   \
+    if (!(cond)) {                       \
+      ::zkb::set_error(__VA_ARGS__);     \
+      return ZKB_ERR_INVALID;            \
+    }                                    \
+  } while (0)
+
+// A cached device table (twiddles, coset factors).  Owned by the context.
+struct DeviceTable {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
+// One per CUDA device: caches shared by every stream on that device.
+struct DeviceContext {
+  int device = -1;
+  int sm_count = 0;
+  std::mutex mu;
+  std::map<std::tuple<int, int, int>, DeviceTable> twiddles;           // (field, log_n, inverse)
+  std::map<std::tuple<int, int, int, uint64_t>, DeviceTable> cosets;   // (field, log_n, log_b, shift)
+};
+
+// Context of the calling thread's current device (initialised on first use).
+int current_context(DeviceContext **out);
+// Stream of the calling thread on its current device (created on first use).
+cudaStream_t thread_stream();
+// A user stream argument follows CUDA's convention: NULL is the default stream.
+inline cudaStream_t resolve_stream(void *s) { return (cudaStream_t)s; }
+
+// Stream-ordered scratch allocation from the device's memory pool.
+int dev_alloc(void **p, size_t bytes, cudaStream_t s);
+void dev_free(void *p, cudaStream_t s);
+
+// RAII holder for stream-ordered scratch.
+struct ScratchBuf {
+  void *p = nullptr;
+  cudaStream_t s = nullptr;
+  ScratchBuf() = default;
+  ScratchBuf(const ScratchBuf &) = delete;
+  ScratchBuf &operator=(const ScratchBuf &) = delete;
+  ~ScratchBuf() {
+    if (p) dev_free(p, s);
+  }
+  int alloc(size_t bytes, cudaStream_t stream) {
+    s = stream;
+    return dev_alloc(&p, bytes ? bytes : 16, stream);
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+inline size_t field_elem_bytes(int field) { return field == ZKB_FIELD_BABYBEAR ? 4 : 8; }
+
+inline int ilog2_exact(uint64_t x) {
+  int l = 0;
+  while ((1ull << l) < x) l++;
+  return (1ull << l) == x ? l : -1;
+}
+
+inline uint64_t ceil_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+inline unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 148u * 64u) {
+  uint64_t g = (n + threads - 1) / threads;
+  if (g == 0) g = 1;
+  return (unsigned)(g < cap ? g : cap);
+}
+
+}  // namespace zkb

@@ -1,0 +1,66 @@
+// engine.cuh — internal host-side interfaces between the CUDA modules.
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+#include "p2_consts.h"
+#include "poseidon2.cuh"
+
+namespace zkb {
+
+// --------------------------------------------------------------- poseidon2.cu
+template <class F, int W>
+bool build_p2_params(const uint64_t *rc, size_t n_rc, int rounds_f, int rounds_p,
+                     const uint64_t *diag, int out, P2Params<F, W> *p);
+template <class F, int W>
+bool build_p2_params(const HasherSpec &h, P2Params<F, W> *p);
+template <class F, int W>
+int p2_permute_batch(typename F::T *d_states, size_t n_states, const P2Params<F, W> &p,
+                     cudaStream_t s);
+
+// --------------------------------------------------------------------- ntt.cu
+// Column-wise natural-order DFT of a row-major 2^log_h x width matrix, in place.
+template <class F>
+int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaStream_t s);
+// p3 coset_lde_batch (+ bit_reverse_rows when bitrev): d_out holds 2^(log_h+log_b) rows.
+template <class F>
+int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log_b,
+                typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s);
+// Cached table of w^t (t < 2^log_n) for w = two_adic_generator(log_n)^(+-1), encoded
+// for Field::mul_tw (Montgomery form for BabyBear).
+template <class F>
+int get_twiddles(int log_n, bool inverse, const typename F::T **out, cudaStream_t s);
+
+// ------------------------------------------------------------------ merkle.cu
+struct TreeMatrix {
+  const void *data;  // device pointer, row-major
+  uint64_t height;
+  uint64_t width;
+};
+
+struct DeviceTree {
+  HasherSpec spec;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  void *d_layers = nullptr;                 // every digest layer, back to back
+  std::vector<uint64_t> layer_off;          // in digests
+  std::vector<uint64_t> layer_len;          // in digests
+  std::vector<TreeMatrix> mats;             // commit order
+  std::vector<void *> owned;                // device copies made by host-pointer commits
+  ~DeviceTree();
+};
+
+// p3 MerkleTree::new over device matrices; fills layers and the tree description.
+int mmcs_build_dev(const HasherSpec &h, const std::vector<TreeMatrix> &mats, DeviceTree *tree,
+                   cudaStream_t s);
+// Copy the root (spec.out elements) to host memory (synchronises the stream).
+int mmcs_root_to_host(const DeviceTree *tree, void *root_out, cudaStream_t s);
+
+// --------------------------------------------------------------------- fri.cu
+template <class F>
+int fri_fold_base_dev(const typename F::T *d_evals, size_t n_out, typename F::T alpha,
+                      const typename F::T *d_inv_tw, typename F::T *d_out, cudaStream_t s);
+int fri_fold_ext4_dev(const uint32_t *d_evals, size_t n_out, const uint32_t beta[4],
+                      uint32_t *d_out, cudaStream_t s);
+
+}  // namespace zkb

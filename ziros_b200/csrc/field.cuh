@@ -1,0 +1,171 @@
+// field.cuh — BabyBear and Goldilocks arithmetic for sm_100a.
+//
+// BabyBear (p = 2^31 - 2^27 + 1) uses 32-bit Montgomery multiplication with
+// R = 2^32: four 32-bit multiplies (lo, hi, lo, hi) and a conditional add.
+// Goldilocks (p = 2^64 - 2^32 + 1) uses the special-form reduction
+// 2^64 = 2^32 - 1 (mod p) of the 128-bit product.
+//
+// Reference semantics: zkf-metal/src/shaders/field_babybear.metal:1-25 and
+// field_goldilocks.metal:1-56.  Every value that leaves a kernel is canonical.
+#pragma once
+#include <cstdint>
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#endif
+
+namespace zkb {
+
+// ----------------------------------------------------------------- BabyBear
+struct BabyBear {
+  using T = uint32_t;
+  static constexpr uint32_t P = 0x78000001u;
+  // p^-1 mod 2^32: p = 1 + 15*2^27, so p^-1 = 1 - 15*2^27 (the square term vanishes).
+  static constexpr uint32_t PINV = 0x88000001u;
+  static constexpr uint32_t R2 = 0x45dddde3u;  // 2^64 mod p (to-Montgomery factor)
+  static constexpr uint32_t ONE_MONT = 0x0ffffffeu;  // 2^32 mod p
+  static constexpr int TWO_ADICITY = 27;
+  static constexpr uint32_t GENERATOR = 31;
+
+  __host__ __device__ __forceinline__ static uint32_t add(uint32_t a, uint32_t b) {
+    uint32_t s = a + b;
+    uint32_t t = s - P;
+    return s < P ? s : t;
+  }
+  __host__ __device__ __forceinline__ static uint32_t sub(uint32_t a, uint32_t b) {
+    uint32_t d = a - b;
+    return a >= b ? d : d + P;
+  }
+  __host__ __device__ __forceinline__ static uint32_t neg(uint32_t a) { return a ? P - a : 0; }
+  // Montgomery product a*b*2^-32 mod p for a*b < p*2^32 (both < p suffices).
+  __host__ __device__ __forceinline__ static uint32_t mont(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+    uint32_t lo = a * b;
+    uint32_t hi = __umulhi(a, b);
+    uint32_t m = lo * PINV;
+    uint32_t mp = __umulhi(m, P);
+#else
+    uint64_t t = (uint64_t)a * b;
+    uint32_t lo = (uint32_t)t, hi = (uint32_t)(t >> 32);
+    uint32_t m = lo * PINV;
+    uint32_t mp = (uint32_t)(((uint64_t)m * P) >> 32);
+#endif
+    uint32_t r = hi - mp;
+    return hi < mp ? r + P : r;
+  }
+  __host__ __device__ __forceinline__ static uint32_t to_mont(uint32_t a) { return mont(a, R2); }
+  __host__ __device__ __forceinline__ static uint32_t from_mont(uint32_t a) { return mont(a, 1); }
+  // Canonical x times a twiddle stored in Montgomery form -> canonical product.
+  __host__ __device__ __forceinline__ static uint32_t mul_tw(uint32_t x, uint32_t w_mont) {
+    return mont(x, w_mont);
+  }
+  // Host-side plain product (tables, constants).
+  static inline uint32_t mul_host(uint32_t a, uint32_t b) {
+    return (uint32_t)(((uint64_t)a * b) % P);
+  }
+  // Encoding of a canonical twiddle for mul_tw.
+  static inline uint32_t tw_encode(uint32_t w) { return (uint32_t)(((uint64_t)w << 32) % P); }
+};
+
+// --------------------------------------------------------------- Goldilocks
+struct Goldilocks {
+  using T = uint64_t;
+  static constexpr uint64_t P = 0xFFFFFFFF00000001ull;
+  static constexpr uint64_t EPS = 0xFFFFFFFFull;  // 2^64 - p
+  static constexpr int TWO_ADICITY = 32;
+  static constexpr uint64_t GENERATOR = 7;
+
+  __host__ __device__ __forceinline__ static uint64_t canon(uint64_t x) {
+    return x >= P ? x - P : x;
+  }
+  __host__ __device__ __forceinline__ static uint64_t add(uint64_t a, uint64_t b) {
+    uint64_t s = a + b;
+    // carry out of 2^64: 2^64 = EPS (mod p); the sum of two canonical values stays < 2^64 after it
+    if (s < a) s += EPS;
+    return canon(s);
+  }
+  __host__ __device__ __forceinline__ static uint64_t sub(uint64_t a, uint64_t b) {
+    uint64_t d = a - b;
+    if (a < b) d -= EPS;  // d + 2^64 - EPS = a - b + p
+    return d;
+  }
+  __host__ __device__ __forceinline__ static uint64_t neg(uint64_t a) { return a ? P - a : 0; }
+  // Reduce hi*2^64 + lo: 2^64 = 2^32 - 1 and 2^96 = -1 (mod p).
+  __host__ __device__ __forceinline__ static uint64_t reduce128(uint64_t lo, uint64_t hi) {
+    uint64_t hi_hi = hi >> 32, hi_lo = hi & 0xFFFFFFFFull;
+    uint64_t t0 = lo - hi_hi;
+    if (lo < hi_hi) t0 -= EPS;
+    uint64_t t1 = hi_lo * EPS;
+    uint64_t r = t0 + t1;
+    if (r < t1) r += EPS;
+    return canon(r);
+  }
+  __host__ __device__ __forceinline__ static uint64_t mul(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+    uint64_t lo = a * b, hi = __umul64hi(a, b);
+#else
+    unsigned __int128 t = (unsigned __int128)a * b;
+    uint64_t lo = (uint64_t)t, hi = (uint64_t)(t >> 64);
+#endif
+    return reduce128(lo, hi);
+  }
+  __host__ __device__ __forceinline__ static uint64_t mul_tw(uint64_t x, uint64_t w) { return mul(x, w); }
+  static inline uint64_t mul_host(uint64_t a, uint64_t b) { return mul(a, b); }
+  static inline uint64_t tw_encode(uint64_t w) { return w; }
+};
+
+// "Encoded" domain used for twiddles, coset factors and Poseidon2 state:
+// Montgomery form for BabyBear (products are single Montgomery multiplications),
+// canonical for Goldilocks.
+template <class F>
+struct Dom;
+
+template <>
+struct Dom<BabyBear> {
+  using T = uint32_t;
+  __host__ __device__ __forceinline__ static T enter(T x) { return BabyBear::to_mont(x); }
+  __host__ __device__ __forceinline__ static T leave(T x) { return BabyBear::from_mont(x); }
+  __host__ __device__ __forceinline__ static T mul(T a, T b) { return BabyBear::mont(a, b); }
+  __host__ __device__ __forceinline__ static T add(T a, T b) { return BabyBear::add(a, b); }
+  __host__ __device__ __forceinline__ static T sub(T a, T b) { return BabyBear::sub(a, b); }
+  static inline T encode(uint64_t canonical) { return BabyBear::tw_encode((uint32_t)canonical); }
+  static constexpr T ONE = BabyBear::ONE_MONT;
+};
+
+template <>
+struct Dom<Goldilocks> {
+  using T = uint64_t;
+  __host__ __device__ __forceinline__ static T enter(T x) { return x; }
+  __host__ __device__ __forceinline__ static T leave(T x) { return x; }
+  __host__ __device__ __forceinline__ static T mul(T a, T b) { return Goldilocks::mul(a, b); }
+  __host__ __device__ __forceinline__ static T add(T a, T b) { return Goldilocks::add(a, b); }
+  __host__ __device__ __forceinline__ static T sub(T a, T b) { return Goldilocks::sub(a, b); }
+  static inline T encode(uint64_t canonical) { return canonical; }
+  static constexpr T ONE = 1;
+};
+
+template <class F>
+static inline typename F::T pow_host(typename F::T a, uint64_t e) {
+  typename F::T r = 1, b = a;
+  while (e) {
+    if (e & 1) r = F::mul_host(r, b);
+    b = F::mul_host(b, b);
+    e >>= 1;
+  }
+  return r;
+}
+template <class F>
+static inline typename F::T inv_host(typename F::T a) {
+  return pow_host<F>(a, (uint64_t)F::P - 2);
+}
+// two_adic_generator(bits) = (g^((p-1)/2^S))^(2^(S-bits)).
+template <class F>
+static inline typename F::T two_adic_generator(int bits) {
+  typename F::T root = pow_host<F>(F::GENERATOR, ((uint64_t)F::P - 1) >> F::TWO_ADICITY);
+  for (int i = bits; i < F::TWO_ADICITY; i++) root = F::mul_host(root, root);
+  return root;
+}
+
+}  // namespace zkb

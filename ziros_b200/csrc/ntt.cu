@@ -1,0 +1,368 @@
+// ntt.cu — column-batched NTT and coset low-degree extension on row-major matrices.
+//
+// Reference path: MetalDft::dft_batch / idft_batch (zkf-metal/src/ntt/p3_adapter.rs:69-459)
+// and p3's default coset_lde_batch + the PCS's bit_reverse_rows
+// (zkf-backends/src/plonky3.rs:250-262, stark_to_groth16.rs:2324-2346).  The
+// reference runs one HBM pass per radix-2 stage after a host bit-reversal; here a
+// transform of size 2^L is cut into a few passes of 2^k-point sub-DFTs staged in
+// shared memory (four-step decomposition, applied recursively):
+//
+//   pass over index bits [lo, hi):  for every fixed value of the other bits, the
+//   2^k elements x[t] at rows base + t*2^lo get Y[f] = sum_t x[t] w_{2^k}^{tf}
+//   (radix-2 decimation in frequency, natural in / bit-reversed out), then the
+//   twist Y[f] *= w_{2^hi}^{(row mod 2^lo) * f}, stored back at rows
+//   base + rev_k(f)*2^lo.
+//
+// Passes run from the top bits down, so the final layout is the bit-reversed
+// (natural-in, reversed-out) DFT.  That is exactly the row order the PCS commits,
+// so the LDE needs no separate bit-reversal:
+//
+//   LDE_bitrev[r*n + q] = DFT_n( c_m * (s * w_{bn}^{j})^m )[rev(q)],  j = rev_b(r),
+//
+// i.e. b independent size-n NR transforms of the coefficients twisted per coset.
+#include <algorithm>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "field.cuh"
+
+namespace zkb {
+
+// ------------------------------------------------------------------ tables
+template <class F>
+struct PowParams {
+  typename F::T b2[40];  // encoded base^(2^j)
+  typename F::T scale;   // encoded
+};
+
+// out[t] = scale * base^t (encoded domain), product of the base^(2^j) for the set bits of t.
+template <class F>
+__global__ void powers_kernel(typename F::T *out, uint64_t n, const __grid_constant__ PowParams<F> pp) {
+  using D = Dom<F>;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    typename F::T acc = pp.scale;
+    uint64_t e = t;
+    int j = 0;
+    while (e) {
+      if (e & 1) acc = D::mul(acc, pp.b2[j]);
+      e >>= 1;
+      j++;
+    }
+    out[t] = acc;
+  }
+}
+
+template <class F>
+static int launch_powers(typename F::T *out, uint64_t n, typename F::T base, typename F::T scale,
+                         cudaStream_t s) {
+  PowParams<F> pp;
+  typename F::T b = base;
+  for (int j = 0; j < 40; j++) {
+    pp.b2[j] = Dom<F>::encode(b);
+    b = F::mul_host(b, b);
+  }
+  pp.scale = Dom<F>::encode(scale);
+  powers_kernel<F><<<grid_for(n, 256), 256, 0, s>>>(out, n, pp);
+  ZKB_CHECK_LAUNCH();
+  return ZKB_OK;
+}
+
+template <class F>
+static constexpr int field_id() {
+  return sizeof(typename F::T) == 4 ? ZKB_FIELD_BABYBEAR : ZKB_FIELD_GOLDILOCKS;
+}
+
+template <class F>
+int get_twiddles(int log_n, bool inverse, const typename F::T **out, cudaStream_t s) {
+  using T = typename F::T;
+  DeviceContext *ctx;
+  ZKB_TRY(current_context(&ctx));
+  if (log_n > F::TWO_ADICITY) {
+    set_error("NTT size 2^%d exceeds the two-adicity of the field", log_n);
+    return ZKB_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto key = std::make_tuple(field_id<F>(), log_n, (int)inverse);
+  auto it = ctx->twiddles.find(key);
+  if (it != ctx->twiddles.end()) {
+    *out = (const T *)it->second.ptr;
+    return ZKB_OK;
+  }
+  uint64_t n = 1ull << log_n;
+  void *p = nullptr;
+  ZKB_CHECK_CUDA(cudaMalloc(&p, n * sizeof(T)));
+  T w = two_adic_generator<F>(log_n);
+  if (inverse) w = inv_host<F>(w);
+  int rc = launch_powers<F>((T *)p, n, w, 1, s);
+  if (rc == ZKB_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = ZKB_ERR_CUDA;
+  if (rc != ZKB_OK) {
+    cudaFree(p);
+    return rc;
+  }
+  ctx->twiddles[key] = DeviceTable{p, n * sizeof(T)};
+  *out = (const T *)p;
+  return ZKB_OK;
+}
+
+// Coset factors: tab[j*n + m] = (shift * w_{bn}^j)^m / n, encoded.
+template <class F>
+static int get_coset_table(int log_n, int log_b, typename F::T shift, const typename F::T **out,
+                           cudaStream_t s) {
+  using T = typename F::T;
+  DeviceContext *ctx;
+  ZKB_TRY(current_context(&ctx));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto key = std::make_tuple(field_id<F>(), log_n, log_b, (uint64_t)shift);
+  auto it = ctx->cosets.find(key);
+  if (it != ctx->cosets.end()) {
+    *out = (const T *)it->second.ptr;
+    return ZKB_OK;
+  }
+  uint64_t n = 1ull << log_n, b = 1ull << log_b;
+  void *p = nullptr;
+  ZKB_CHECK_CUDA(cudaMalloc(&p, n * b * sizeof(T)));
+  T w_bn = two_adic_generator<F>(log_n + log_b);
+  T n_inv = inv_host<F>((T)(n % (uint64_t)F::P));
+  T wj = 1;
+  int rc = ZKB_OK;
+  for (uint64_t j = 0; j < b && rc == ZKB_OK; j++) {
+    rc = launch_powers<F>((T *)p + j * n, n, F::mul_host(shift, wj), n_inv, s);
+    wj = F::mul_host(wj, w_bn);
+  }
+  if (rc == ZKB_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = ZKB_ERR_CUDA;
+  if (rc != ZKB_OK) {
+    cudaFree(p);
+    return rc;
+  }
+  ctx->cosets[key] = DeviceTable{p, n * b * sizeof(T)};
+  *out = (const T *)p;
+  return ZKB_OK;
+}
+
+// -------------------------------------------------------------- pass kernel
+struct PassGeom {
+  int L;                     // log2 of each transform
+  int lo, k;                 // index bits [lo, lo+k)
+  uint32_t width;            // matrix columns
+  uint32_t cols;             // columns per CTA (power of two dividing width)
+  int log_cols;
+  uint32_t chunks_per_row;   // width / cols
+  uint32_t groups;           // 2^(L-k) groups per transform
+  uint64_t block_stride;     // elements between transforms
+  int twist;
+};
+
+template <class F>
+__global__ void __launch_bounds__(256)
+    ntt_pass_kernel(const typename F::T *in, typename F::T *out, const PassGeom g,
+                    const typename F::T *__restrict__ tw, typename F::T post_scale) {
+  using T = typename F::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *tile = reinterpret_cast<T *>(smem_raw);
+  const int k = g.k;
+  const int n_sub = 1 << k;
+  T *tws = tile + ((size_t)n_sub << g.log_cols);
+
+  const uint64_t cta = blockIdx.x;
+  const uint32_t chunk = (uint32_t)(cta % g.chunks_per_row);
+  const uint64_t rest = cta / g.chunks_per_row;
+  const uint32_t grp = (uint32_t)(rest % g.groups);
+  const uint64_t blk = rest / g.groups;
+  const int hi = g.lo + k;
+  const uint32_t i_low = grp & ((1u << g.lo) - 1u);
+  const uint64_t base_row = ((uint64_t)(grp >> g.lo) << hi) | i_low;
+  const size_t off = blk * g.block_stride + (size_t)chunk * g.cols;
+  const uint32_t C = g.cols, lc = g.log_cols;
+
+  for (int j = threadIdx.x; j < n_sub / 2; j += blockDim.x) tws[j] = tw[(size_t)j << (g.L - k)];
+  for (uint32_t e = threadIdx.x; e < ((uint32_t)n_sub << lc); e += blockDim.x) {
+    uint32_t t = e >> lc, c = e & (C - 1);
+    tile[e] = in[off + ((base_row + ((uint64_t)t << g.lo)) * g.width) + c];
+  }
+  __syncthreads();
+  for (int s = k - 1; s >= 0; s--) {
+    const int half = 1 << s;
+    for (uint32_t e = threadIdx.x; e < ((uint32_t)(n_sub / 2) << lc); e += blockDim.x) {
+      uint32_t p = e >> lc, c = e & (C - 1);
+      uint32_t j = p & (half - 1);
+      uint32_t i0 = ((p >> s) << (s + 1)) | j;
+      T a = tile[(i0 << lc) + c], b = tile[((i0 + half) << lc) + c];
+      tile[(i0 << lc) + c] = F::add(a, b);
+      tile[((i0 + half) << lc) + c] = F::mul_tw(F::sub(a, b), tws[j << (k - 1 - s)]);
+    }
+    __syncthreads();
+  }
+  for (uint32_t e = threadIdx.x; e < ((uint32_t)n_sub << lc); e += blockDim.x) {
+    uint32_t t = e >> lc, c = e & (C - 1);
+    T v = tile[e];
+    if (g.twist) {
+      uint64_t f = __brev(t) >> (32 - k);
+      uint64_t ex = ((uint64_t)i_low * f) & ((1ull << hi) - 1);
+      v = F::mul_tw(v, tw[ex << (g.L - hi)]);
+    }
+    if (post_scale) v = F::mul_tw(v, post_scale);
+    out[off + ((base_row + ((uint64_t)t << g.lo)) * g.width) + c] = v;
+  }
+}
+
+template <class F>
+static uint32_t pick_cols(uint32_t width) {
+  uint32_t cmax = sizeof(typename F::T) == 4 ? 16 : 8;
+  uint32_t c = 1;
+  while (c * 2 <= cmax && width % (c * 2) == 0) c *= 2;
+  return c;
+}
+
+// Split L bits into passes of at most kmax bits, as even as possible, top first.
+static std::vector<int> plan_passes(int L, int kmax) {
+  std::vector<int> ks;
+  if (L <= 0) return ks;
+  int np = (L + kmax - 1) / kmax;
+  for (int i = 0; i < np; i++) ks.push_back(L / np + (i < L % np ? 1 : 0));
+  return ks;
+}
+
+template <class F>
+static int run_passes(const typename F::T *in, typename F::T *out, int L, uint32_t width,
+                      uint64_t n_blocks, const typename F::T *tw, typename F::T last_scale,
+                      cudaStream_t s) {
+  using T = typename F::T;
+  const uint32_t C = pick_cols<F>(width);
+  int lc = 0;
+  while ((1u << lc) < C) lc++;
+  // tile of at most 64 KiB
+  int kmax = 0;
+  while (((size_t)sizeof(T) << (kmax + 1 + lc)) <= 65536 && kmax + 1 <= 12) kmax++;
+  std::vector<int> ks = plan_passes(L, kmax);
+  ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<F>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  int hi = L;
+  const T *src = in;
+  for (size_t pi = 0; pi < ks.size(); pi++) {
+    PassGeom g;
+    g.L = L;
+    g.k = ks[pi];
+    g.lo = hi - g.k;
+    g.width = width;
+    g.cols = C;
+    g.log_cols = lc;
+    g.chunks_per_row = width / C;
+    g.groups = 1u << (L - g.k);
+    g.block_stride = ((uint64_t)width) << L;
+    g.twist = g.lo > 0;
+    uint64_t ctas = (uint64_t)g.chunks_per_row * g.groups * n_blocks;
+    if (ctas >= (1ull << 31)) {
+      set_error("NTT launch too large");
+      return ZKB_ERR_UNSUPPORTED;
+    }
+    size_t smem = (((size_t)1 << g.k) << lc) * sizeof(T) + ((size_t)1 << (g.k - 1)) * sizeof(T);
+    T scale = (pi + 1 == ks.size()) ? last_scale : (T)0;
+    ntt_pass_kernel<F><<<(unsigned)ctas, 256, smem, s>>>(src, out, g, tw, scale);
+    ZKB_CHECK_LAUNCH();
+    src = out;
+    hi = g.lo;
+  }
+  return ZKB_OK;
+}
+
+// ------------------------------------------------------- auxiliary kernels
+template <class F>
+__global__ void bitrev_rows_kernel(const typename F::T *__restrict__ in, typename F::T *__restrict__ out,
+                                   int L, uint32_t width, uint64_t total) {
+  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t row = idx / width, c = idx - row * width;
+    uint64_t r = L ? (__brevll(row) >> (64 - L)) : 0;
+    out[r * width + c] = in[idx];
+  }
+}
+
+// Coefficients in bit-reversed row order -> b twisted copies in natural order.
+template <class F>
+__global__ void lde_expand_kernel(const typename F::T *__restrict__ coef, typename F::T *__restrict__ out,
+                                  int L, int log_b, uint32_t width,
+                                  const typename F::T *__restrict__ ctab) {
+  const uint64_t n = 1ull << L, total = n * width;
+  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t m = idx / width, c = idx - m * width;
+    uint64_t src = L ? (__brevll(m) >> (64 - L)) : 0;
+    typename F::T v = coef[src * width + c];
+    for (uint32_t r = 0; r < (1u << log_b); r++) {
+      uint32_t j = log_b ? (__brev(r) >> (32 - log_b)) : 0;
+      out[(((uint64_t)r << L) + m) * width + c] = F::mul_tw(v, ctab[((uint64_t)j << L) + m]);
+    }
+  }
+}
+
+// ----------------------------------------------------------------- drivers
+template <class F>
+int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaStream_t s) {
+  using T = typename F::T;
+  if (width == 0 || log_h == 0) return ZKB_OK;
+  const T *tw;
+  ZKB_TRY(get_twiddles<F>(log_h, inverse, &tw, s));
+  uint64_t n = 1ull << log_h;
+  ScratchBuf tmp;
+  ZKB_TRY(tmp.alloc(n * width * sizeof(T), s));
+  T scale = 0;
+  if (inverse) scale = Dom<F>::encode(inv_host<F>((T)(n % (uint64_t)F::P)));
+  ZKB_TRY(run_passes<F>(d, tmp.as<T>(), log_h, width, 1, tw, scale, s));
+  bitrev_rows_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(tmp.as<T>(), d, log_h, width,
+                                                                   n * width);
+  ZKB_CHECK_LAUNCH();
+  return ZKB_OK;
+}
+
+template <class F>
+int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log_b,
+                typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s) {
+  using T = typename F::T;
+  if (width == 0) return ZKB_OK;
+  if (log_h + log_b > F::TWO_ADICITY) {
+    set_error("LDE size 2^%d exceeds the two-adicity of the field", log_h + log_b);
+    return ZKB_ERR_INVALID;
+  }
+  const uint64_t n = 1ull << log_h;
+  ScratchBuf coef;
+  ZKB_TRY(coef.alloc(n * width * sizeof(T), s));
+  if (log_h > 0) {
+    const T *itw;
+    ZKB_TRY(get_twiddles<F>(log_h, true, &itw, s));
+    ZKB_TRY(run_passes<F>(d_trace, coef.as<T>(), log_h, width, 1, itw, (T)0, s));
+  } else {
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(coef.p, d_trace, width * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  }
+  const T *ctab;
+  ZKB_TRY(get_coset_table<F>(log_h, log_b, shift, &ctab, s));
+  lde_expand_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(coef.as<T>(), d_out, log_h, log_b,
+                                                                  width, ctab);
+  ZKB_CHECK_LAUNCH();
+  if (log_h > 0) {
+    const T *tw;
+    ZKB_TRY(get_twiddles<F>(log_h, false, &tw, s));
+    ZKB_TRY(run_passes<F>(d_out, d_out, log_h, width, 1ull << log_b, tw, (T)0, s));
+  }
+  if (!bitrev) {
+    const int LN = log_h + log_b;
+    const uint64_t total = (n << log_b) * width;
+    ScratchBuf tmp;
+    ZKB_TRY(tmp.alloc(total * sizeof(T), s));
+    bitrev_rows_kernel<F><<<grid_for(total, 256), 256, 0, s>>>(d_out, tmp.as<T>(), LN, width, total);
+    ZKB_CHECK_LAUNCH();
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(d_out, tmp.p, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  }
+  return ZKB_OK;
+}
+
+template int get_twiddles<BabyBear>(int, bool, const uint32_t **, cudaStream_t);
+template int get_twiddles<Goldilocks>(int, bool, const uint64_t **, cudaStream_t);
+template int ntt_dft_dev<BabyBear>(uint32_t *, int, uint32_t, bool, cudaStream_t);
+template int ntt_dft_dev<Goldilocks>(uint64_t *, int, uint32_t, bool, cudaStream_t);
+template int ntt_lde_dev<BabyBear>(const uint32_t *, int, uint32_t, int, uint32_t, bool, uint32_t *,
+                                   cudaStream_t);
+template int ntt_lde_dev<Goldilocks>(const uint64_t *, int, uint32_t, int, uint64_t, bool,
+                                     uint64_t *, cudaStream_t);
+
+}  // namespace zkb

@@ -1,0 +1,109 @@
+// poseidon2.cuh — Poseidon2 permutation on the device, one state per thread.
+//
+// Structure (zkf-metal/src/shaders/poseidon2.metal:1-154 and :157-264;
+// zkf-backends/src/wrapping/poseidon2_goldilocks.rs:117-345):
+//   external MDS; R_F/2 full rounds (add rc, x^7 on every lane, external MDS);
+//   R_P partial rounds (add rc + x^7 on lane 0, s_i <- d_i*s_i + sum(s));
+//   R_F/2 full rounds.
+// External MDS = M4 [[2,3,1,1],[1,2,3,1],[1,1,2,3],[3,1,1,2]] on each 4-lane chunk,
+// then every lane adds the sum of its residue class mod 4.
+//
+// The state lives in registers in the "internal domain": Montgomery form for
+// BabyBear (so x^7 and the diagonal products are single Montgomery products),
+// canonical for Goldilocks.  Round constants and the diagonal are passed by value
+// as a kernel parameter, so they sit in the constant bank and every lane of a
+// warp reads the same word (broadcast), which is the access pattern of a
+// permutation that is uniform across threads.
+#pragma once
+#include "field.cuh"
+
+namespace zkb {
+
+template <class F>
+using P2Dom = Dom<F>;
+
+// Largest supported instance: width 16, R_F = 8, R_P = 22.
+constexpr int P2_MAX_RC = 8 * 16 + 22;
+
+template <class F, int W>
+struct P2Params {
+  typename F::T rc[P2_MAX_RC];  // internal-domain constants, flat [initial | internal | terminal]
+  typename F::T diag[W];        // internal-domain diagonal
+  int rounds_f;
+  int rounds_p;
+  int out;   // digest elements (8 for W16, 4 for W12)
+  int rate;  // sponge rate (8)
+};
+
+template <class F>
+__device__ __forceinline__ typename F::T p2_sbox(typename F::T x) {
+  using D = P2Dom<F>;
+  typename F::T x2 = D::mul(x, x);
+  typename F::T x3 = D::mul(x2, x);
+  typename F::T x4 = D::mul(x2, x2);
+  return D::mul(x4, x3);
+}
+
+template <class F, int W>
+__device__ __forceinline__ void p2_ext_mds(typename F::T (&s)[W]) {
+  using D = P2Dom<F>;
+  using T = typename F::T;
+#pragma unroll
+  for (int c = 0; c < W; c += 4) {
+    T a = s[c], b = s[c + 1], x = s[c + 2], y = s[c + 3];
+    T t01 = D::add(a, b), t23 = D::add(x, y), t0123 = D::add(t01, t23);
+    T t01123 = D::add(t0123, b), t01233 = D::add(t0123, y);
+    s[c] = D::add(t01123, t01);
+    s[c + 1] = D::add(t01123, D::add(x, x));
+    s[c + 2] = D::add(t01233, t23);
+    s[c + 3] = D::add(t01233, D::add(a, a));
+  }
+  T sums[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    sums[k] = s[k];
+#pragma unroll
+    for (int c = 4; c < W; c += 4) sums[k] = D::add(sums[k], s[c + k]);
+  }
+#pragma unroll
+  for (int i = 0; i < W; i++) s[i] = D::add(s[i], sums[i & 3]);
+}
+
+template <class F, int W>
+__device__ __forceinline__ void p2_full_round(typename F::T (&s)[W], const typename F::T *rc) {
+  using D = P2Dom<F>;
+#pragma unroll
+  for (int i = 0; i < W; i++) s[i] = p2_sbox<F>(D::add(s[i], rc[i]));
+  p2_ext_mds<F, W>(s);
+}
+
+template <class F, int W>
+__device__ __forceinline__ void p2_partial_round(typename F::T (&s)[W], typename F::T rc,
+                                                 const typename F::T *diag) {
+  using D = P2Dom<F>;
+  using T = typename F::T;
+  s[0] = p2_sbox<F>(D::add(s[0], rc));
+  T sum = s[0];
+#pragma unroll
+  for (int i = 1; i < W; i++) sum = D::add(sum, s[i]);
+#pragma unroll
+  for (int i = 0; i < W; i++) s[i] = D::add(D::mul(s[i], diag[i]), sum);
+}
+
+// The round loops are deliberately not unrolled: one full-round body (16 S-boxes + MDS,
+// ~9 KB of SASS for BabyBear) and one partial-round body keep the permutation inside
+// the instruction cache while many warps run it at different offsets.  Constants are
+// read from the parameter bank with a per-round index (LDC, uniform across the warp).
+template <class F, int W>
+__device__ __forceinline__ void p2_permute(typename F::T (&s)[W], const P2Params<F, W> &p) {
+  const int half = p.rounds_f / 2, rp = p.rounds_p;
+  p2_ext_mds<F, W>(s);
+#pragma unroll 1
+  for (int r = 0; r < half; r++) p2_full_round<F, W>(s, p.rc + r * W);
+#pragma unroll 1
+  for (int r = 0; r < rp; r++) p2_partial_round<F, W>(s, p.rc[half * W + r], p.diag);
+#pragma unroll 1
+  for (int r = 0; r < half; r++) p2_full_round<F, W>(s, p.rc + half * W + rp + r * W);
+}
+
+}  // namespace zkb
