@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark of the polynomial-commitment hot path: trace cells/s committed.
+
+One step commits one synthetic trace the way TwoAdicFriPcs::commit does: coset
+LDE (blowup 2^log_blowup, shift = field generator), rows bit-reversed, Poseidon2
+MMCS over the rows (zkb_pcs_commit).  The default workload is BabyBear
+2^22 rows x 256 columns, blowup 2 — the 2^22 x 256 BabyBear LDE+commit named as
+the target shape; `--workload` selects the others.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value : whole-job cells/s with the trace resident in HBM (CUDA events on the
+        launching stream, max over ranks).
+e2e   : the same metric through the host-pointer call (zkb_pcs_commit) with the
+        trace in pinned host memory, its H2D copy and the root's D2H read inside
+        the timed region.
+--impl reference : the reference CPU path (restated in C, oracle/) on the host
+        cores, on a bounded sample of the same workload.
+N > 1 runs one independent replica per GPU (torchrun; no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BB_P = 0x78000001
+GL_P = 0xFFFFFFFF00000001
+
+WORKLOADS = {
+    # name: field, log_h, width, log_blowup, Poseidon2 width
+    "babybear_2^22x256_b2": dict(field=0, log_h=22, width=256, log_blowup=1, p2w=16),
+    "goldilocks_2^20x64_b4": dict(field=1, log_h=20, width=64, log_blowup=2, p2w=16),
+    "goldilocks_2^20x64_b4_w12": dict(field=1, log_h=20, width=64, log_blowup=2, p2w=12),
+    "babybear_2^14x16_b2": dict(field=0, log_h=14, width=16, log_blowup=1, p2w=16),
+    # a smaller case of the default workload for profiler captures (inputs still > L2)
+    "babybear_2^18x256_b2": dict(field=0, log_h=18, width=256, log_blowup=1, p2w=16),
+}
+DEFAULT_WORKLOAD = "babybear_2^22x256_b2"
+P2_SEED = 42
+TRACE_SEED = 20240607
+METRIC = "trace cells/s committed (LDE+Poseidon2 Merkle+FRI), batched vs plain; p99 ms"
+
+
+def p2_field_muls(field: int, p2w: int) -> int:
+    """Algorithmic field multiplications of one permutation: 4 per S-box (x^7) on
+    R_F*W + R_P lanes, W per internal round for the diagonal."""
+    rf, rp = (8, 13) if field == 0 else (8, 22)
+    return 4 * (rf * p2w + rp) + rp * p2w
+
+
+def perms_of_commit(log_rows: int, width: int) -> tuple[int, int]:
+    rows = 1 << log_rows
+    return rows * ((width + 7) // 8), rows - 1  # leaf sponge perms, compressions
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU legs
+def cpu_commit_sample(wl: dict, log_rows: int, threads: int) -> tuple[float, int]:
+    """Oracle (reference CPU path restated in C) LDE + MMCS commit of a
+    2^log_rows x width sample; returns (seconds, cells)."""
+    import numpy as np
+
+    import oracle as O
+
+    O.build()
+    O.set_threads(threads)
+    rng = np.random.default_rng(TRACE_SEED)
+    if wl["field"] == 0:
+        t = rng.integers(0, BB_P, size=(1 << log_rows, wl["width"]), dtype=np.uint32)
+    else:
+        t = rng.integers(0, GL_P, size=(1 << log_rows, wl["width"]), dtype=np.uint64)
+    h = O.hasher(wl["field"], P2_SEED, wl["p2w"])
+    t0 = time.perf_counter()
+    lde = O.coset_lde(wl["field"], t, wl["log_blowup"])
+    O.mmcs_commit(h, [lde])
+    return time.perf_counter() - t0, t.size
+
+
+def pick_cpu_sample(wl: dict, threads: int, budget_s: float) -> int:
+    """Largest sample height whose commit fits the per-step budget (doubling)."""
+    log_rows = 10
+    dt, _ = cpu_commit_sample(wl, log_rows, threads)
+    while log_rows < wl["log_h"] and dt * 2.2 < budget_s:
+        log_rows += 1
+        dt *= 2.1
+    return log_rows
+
+
+def run_reference(args, wl: dict, rank: int, world: int) -> int:
+    """--impl reference: the reference's CPU path (oracle/ restatement) on host cores."""
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    log_rows = pick_cpu_sample(wl, threads, budget_s=4.0)
+    for _ in range(args.warmup):
+        cpu_commit_sample(wl, log_rows, threads)
+    times = []
+    cells = 0
+    for _ in range(args.steps):
+        dt, cells = cpu_commit_sample(wl, log_rows, threads)
+        times.append(dt)
+    total = sum(times)
+    value = cells * len(times) / total
+    sample = f"2^{log_rows} x {wl['width']} rows x cols of the {args.workload} workload per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32" if wl["field"] == 0 else "u64", "data": "synthetic (seeded uniform field elements)",
+        "config": {"workload": args.workload, "log_rows": wl["log_h"], "width": wl["width"],
+                   "log_blowup": wl["log_blowup"], "poseidon2_width": wl["p2w"]},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU path restated in C (oracle/); the Rust/p3 build of the reference "
+                "cannot be compiled here (no Rust toolchain, p3 0.4.2 crates absent)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------ GPU arm
+def make_trace(torch, wl: dict, device):
+    g = torch.Generator(device=device)
+    g.manual_seed(TRACE_SEED)
+    n, w = 1 << wl["log_h"], wl["width"]
+    if wl["field"] == 0:
+        return torch.randint(0, BB_P, (n, w), dtype=torch.int32, device=device, generator=g)
+    hi = torch.randint(0, 1 << 32, (n, w), dtype=torch.int64, device=device, generator=g)
+    lo = torch.randint(0, 1 << 32, (n, w), dtype=torch.int64, device=device, generator=g)
+    v = (hi << 32) | lo  # uniform 64-bit pattern in int64 storage
+    # reduce into [0, p): values >= p (as unsigned) are shifted down by p = 2^64 - 2^32 + 1
+    eps = (1 << 32) - 1
+    big = (v < 0) & (v >= -(1 << 32) + 1)
+    return torch.where(big, v + eps, v)
+
+
+def load_traffic(workload: str):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(path)).get(workload)
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
+    import numpy as np
+    import torch
+
+    import ziros_b200 as Z
+    from ziros_b200 import _native as N
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    N.check(N.load().zkb_set_device(local_rank))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    field, lb = wl["field"], wl["log_blowup"]
+    n, w = 1 << wl["log_h"], wl["width"]
+    cells = n * w
+    esize = 4 if field == 0 else 8
+    pcs = Z.CudaTwoAdicPcs(field, P2_SEED, lb, wl["p2w"])
+    trace = make_trace(torch, wl, dev)
+    torch.cuda.synchronize()
+    pinned = torch.empty_like(trace, device="cpu").pin_memory()
+    pinned.copy_(trace)
+    root = np.zeros(pcs.mmcs.digest_elems, dtype=np.uint32 if field == 0 else np.uint64)
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- warm-up (builds twiddle/coset tables, fills the memory pool)
+    for _ in range(max(args.warmup, 1)):
+        pcs.commit_dev(trace, want_tree=False, root=root)
+    for _ in range(max(args.warmup, 1)):
+        pcs.commit_ptr(pinned.data_ptr(), n, w, want_tree=False, root=root)
+    root_ref = root.copy()
+
+    # ---- device-resident timed region (trace resident in HBM, > L2: no flush needed)
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    barrier()
+    if sampler:
+        sampler.start()
+        time.sleep(0.4)
+    N.profile_start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        pcs.commit_dev(trace, want_tree=False, root=root)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    kstats = N.profile_stop()
+    clocks = sampler.stop() if sampler else None
+    t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    assert (root == root_ref).all(), "root changed between steps"
+    gpu_launches = sum(v[0] for v in kstats.values())
+
+    # ---- end-to-end timed region (host pinned trace -> root on host, public host call)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pcs.commit_ptr(pinned.data_ptr(), n, w, want_tree=False, root=root)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    assert (root == root_ref).all()
+
+    # ---- integer-multiply ceiling for the Poseidon2 roofline (measured, this GPU)
+    mul_peak = N.measure_mul_peak(field)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    value = cells * args.steps * world / t_dev
+    e2e = cells * args.steps * world / t_e2e
+    # roofline of the dominant kernel (leaf sponge hashing; integer-multiply bound)
+    N_rows = n << lb
+    leaf_perms, comp_perms = perms_of_commit(wl["log_h"] + lb, w)
+    lk = kstats.get("merkle_leaf_hash", (1, float("nan"), 0))
+    leaf_ms = lk[1] / max(lk[0], 1)
+    muls = leaf_perms * p2_field_muls(field, wl["p2w"])
+    achieved = muls / (leaf_ms * 1e-3) / 1e9
+    traffic = load_traffic(args.workload)
+    roofline = {
+        "kernel": "merkle_leaf_hash", "bound": "int", "unit": "Gmul/s",
+        "achieved": achieved, "peak": mul_peak / 1e9, "frac": achieved / (mul_peak / 1e9),
+        "peak_source": "measured in this run: zkb_measure_mul_peak (independent field-multiply chains on all SMs)",
+        "work_per_launch": f"{leaf_perms} Poseidon2 perms x {p2_field_muls(field, wl['p2w'])} field mults",
+        "traffic": traffic.get("merkle_leaf_hash") if traffic else None,
+    }
+    # HBM roofline of the NTT passes (each pass reads and writes its tiles once)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm_peak, hbm_src = float(peaks["hbm_gbs"]), "of measured"
+    except (OSError, ValueError, KeyError):
+        hbm_peak, hbm_src = 6650.0, "of fallback"
+    nk = kstats.get("ntt_pass")
+    ntt_roof = None
+    if nk:
+        n_inv_passes = (wl["log_h"] + 9) // 10
+        n_fwd_passes = n_inv_passes
+        bytes_per_step = 2 * esize * (n * w * n_inv_passes + N_rows * w * n_fwd_passes)
+        per_launch = bytes_per_step * args.steps / nk[0]
+        ach = per_launch / (nk[1] / nk[0] * 1e-3) / 1e9
+        ntt_roof = {"kernel": "ntt_pass", "bound": "hbm", "unit": "GB/s", "achieved": ach, "peak": hbm_peak,
+                    "frac": ach / hbm_peak, "peak_source": hbm_src,
+                    "traffic": traffic.get("ntt_pass") if traffic else None}
+
+    # ---- CPU baseline (oracle on host cores, bounded sample)
+    cpu = None
+    if world == 1 and not args.skip_cpu:
+        threads = os.cpu_count() or 1
+        log_rows = pick_cpu_sample(wl, threads, budget_s=8.0)
+        dts = []
+        for _ in range(2):
+            dt, c = cpu_commit_sample(wl, log_rows, threads)
+            dts.append(dt)
+        cpu = {"value": c / min(dts), "unit": "cells/s", "cores": threads, "kind": "port",
+               "sample": f"2^{log_rows} x {w} trace (LDE x2^{lb} + MMCS), best of 2, oracle/ C restatement"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32" if field == 0 else "u64",
+        "data": "synthetic (seeded uniform field elements)",
+        "config": {"workload": args.workload, "log_rows": wl["log_h"], "width": wl["width"],
+                   "log_blowup": wl["log_blowup"], "poseidon2_width": wl["p2w"],
+                   "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (trace %.1f GB, LDE %.1f GB)" % (cells * esize / 1e9,
+                                                                             N_rows * w * esize / 1e9)},
+        "e2e": {"value": e2e, "unit": "cells/s", "h2d_bytes_per_step": cells * esize,
+                "d2h_bytes_per_step": int(root.nbytes), "ms_per_step": 1e3 * t_e2e / args.steps},
+        "roofline": roofline,
+        "roofline_ntt": ntt_roof,
+        "cpu_baseline": cpu,
+        "gpu_launches": gpu_launches,
+        "kernels": {k: {"launches": v[0], "ms_total": round(v[1], 3), "ms_max": round(v[2], 3)}
+                    for k, v in sorted(kstats.items(), key=lambda kv: -kv[1][1])},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, wl, rank, world)
+    return run_ours(args, wl, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

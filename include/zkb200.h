@@ -61,6 +61,27 @@ ZKB_API int zkb_device_count(void);
 /* Select the device used by this thread's subsequent calls. */
 ZKB_API int zkb_set_device(int device);
 
+/* Kernel timing.  zkb_profile_start() enables per-launch CUDA events (recorded on
+ * the stream each kernel is launched on) and clears earlier records;
+ * zkb_profile_stop() disables them, waits for the events and writes one entry per
+ * kernel name (at most `cap`); returns the number of names.  This is the per-stage
+ * timing hook of the reference's GPU telemetry (zkf-runtime/src/telemetry.rs:1-25,
+ * zkf-backends/src/plonky3.rs:806-971). */
+typedef struct {
+  char name[48];
+  uint64_t launches;
+  double total_ms;
+  double max_ms;
+} zkb_kernel_stat;
+ZKB_API int zkb_profile_start(void);
+ZKB_API int zkb_profile_stop(zkb_kernel_stat *out, int cap);
+
+/* Measured field-multiplication ceiling of the current device: field
+ * multiplications per second of independent multiply chains on every SM (the
+ * integer-pipe roofline of the Poseidon2 kernels).  No reference counterpart: it
+ * is this library's measurement hook. */
+ZKB_API int zkb_measure_mul_peak(int field, double *mul_per_s);
+
 /* ---------------------------------------------------------------- Poseidon2 */
 /* flatten_round_constants(seed) (zkf-metal/src/poseidon2/babybear.rs:76-111,
  * goldilocks.rs:42-83).  Writes up to `cap` canonical constants in the layout
@@ -155,6 +176,21 @@ ZKB_API int zkb_tree_copy_layer(const zkb_tree *tree, int layer, void *host_out)
 ZKB_API int zkb_mmcs_open_batch(const zkb_tree *tree, uint64_t index, void *rows_out, size_t rows_cap,
                         void *siblings_out, size_t siblings_cap);
 ZKB_API void zkb_tree_free(zkb_tree *tree);
+
+/* TwoAdicFriPcs::commit for one trace matrix (the PCS type of
+ * zkf-backends/src/plonky3.rs:68): coset LDE with shift = field generator, rows
+ * bit-reversed, MMCS commit of the result — coset_lde_batch + bit_reverse_rows +
+ * Mmcs::commit in one call.  The LDE (2^(log_h+log_blowup) x width) stays on the
+ * device as the tree's leaf matrix, so openings read it without a copy.
+ * Host form: `trace` is a host pointer (pinned memory gives full copy bandwidth). */
+ZKB_API int zkb_pcs_commit(const zkb_hasher *hasher, const void *trace, uint32_t log_h,
+                           uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out);
+ZKB_API int zkb_pcs_commit_dev(const zkb_hasher *hasher, const void *d_trace, uint32_t log_h,
+                               uint32_t width, uint32_t log_blowup, void *root_out,
+                               zkb_tree **tree_out, void *stream);
+/* Device pointer to the committed leaf matrix `mat` of a tree (for device-resident
+ * follow-up work such as the FRI input); NULL on error. */
+ZKB_API const void *zkb_tree_matrix_dev(const zkb_tree *tree, int mat);
 
 /* ---------------------------------------------------------------------- FRI */
 /* FriAccelerator::fold_goldilocks (zkf-core/src/acceleration.rs:197-217) and

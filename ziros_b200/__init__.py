@@ -12,6 +12,7 @@ from .accel import (  # noqa: F401
     CudaFri,
     CudaMerkleTreeMmcs,
     CudaPoseidon2,
+    CudaTwoAdicPcs,
     Tree,
     round_constants,
 )

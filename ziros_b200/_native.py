@@ -42,6 +42,11 @@ class Matrix(C.Structure):
     _fields_ = [("data", C.c_void_p), ("height", C.c_uint64), ("width", C.c_uint64)]
 
 
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("launches", C.c_uint64), ("total_ms", C.c_double),
+                ("max_ms", C.c_double)]
+
+
 class Hasher(C.Structure):
     _fields_ = [("field", C.c_int), ("width", C.c_uint32), ("seed", C.c_uint64)]
 
@@ -57,6 +62,9 @@ SIGNATURES = {
     "zkb_last_error_message": (C.c_char_p, []),
     "zkb_device_count": (_I, []),
     "zkb_set_device": (_I, [_I]),
+    "zkb_measure_mul_peak": (_I, [_I, _P]),
+    "zkb_profile_start": (_I, []),
+    "zkb_profile_stop": (_I, [_P, _I]),
     "zkb_poseidon2_babybear_round_constants": (_I, [_U64, _P, _SZ, _P, _P]),
     "zkb_poseidon2_goldilocks_round_constants": (_I, [_U64, _U32, _P, _SZ, _P, _P]),
     "zkb_poseidon2_babybear_permute": (_I, [_P, _SZ, _P, _SZ, _U32, _U32]),
@@ -69,6 +77,9 @@ SIGNATURES = {
     "zkb_coset_lde_batch_dev": (_I, [_I, _P, _U32, _U32, _U32, _U64, _I, _P, _P]),
     "zkb_mmcs_commit": (_I, [_P, _P, _SZ, _P, _P]),
     "zkb_mmcs_commit_dev": (_I, [_P, _P, _SZ, _P, _P, _P]),
+    "zkb_pcs_commit": (_I, [_P, _P, _U32, _U32, _U32, _P, _P]),
+    "zkb_pcs_commit_dev": (_I, [_P, _P, _U32, _U32, _U32, _P, _P, _P]),
+    "zkb_tree_matrix_dev": (_P, [_P, _I]),
     "zkb_tree_num_layers": (_I, [_P]),
     "zkb_tree_layer_len": (C.c_int64, [_P, _I]),
     "zkb_tree_digest_elems": (_I, [_P]),
@@ -116,6 +127,26 @@ def check(rc: int) -> int:
     if rc == DECLINED:
         raise ZkbDeclined(rc, last_error())
     raise ZkbError(rc, last_error())
+
+
+def profile_start() -> None:
+    check(load().zkb_profile_start())
+
+
+def profile_stop() -> dict:
+    """{kernel name: (launches, total_ms, max_ms)} since profile_start()."""
+    buf = (KernelStat * 64)()
+    n = load().zkb_profile_stop(buf, 64)
+    check(n if n < 0 else 0)
+    return {buf[i].name.decode(): (int(buf[i].launches), float(buf[i].total_ms), float(buf[i].max_ms))
+            for i in range(min(n, 64))}
+
+
+def measure_mul_peak(field: int) -> float:
+    """Field multiplications per second of the device's multiply pipe (see diag.cu)."""
+    v = C.c_double()
+    check(load().zkb_measure_mul_peak(field, C.byref(v)))
+    return float(v.value)
 
 
 def device_count() -> int:

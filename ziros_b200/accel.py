@@ -163,11 +163,11 @@ class CudaDft:
 class Tree:
     """Prover data of a commitment (p3 MerkleTree): digest layers stay on the device."""
 
-    def __init__(self, handle: C.c_void_p, field: int, mats: Sequence[np.ndarray]):
+    def __init__(self, handle: C.c_void_p, field: int, shapes: Sequence[Tuple[int, int]]):
         self._h = handle
         self.field = field
-        self.widths = [m.shape[1] for m in mats]
-        self.heights = [m.shape[0] for m in mats]
+        self.heights = [int(s[0]) for s in shapes]
+        self.widths = [int(s[1]) for s in shapes]
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -214,7 +214,7 @@ class CudaMerkleTreeMmcs:
         root = np.zeros(self.digest_elems, dtype=dt)
         handle = C.c_void_p()
         N.check(N.load().zkb_mmcs_commit(C.byref(self.hasher), descs, len(mats), _ptr(root), C.byref(handle)))
-        return root, Tree(handle, self.field, mats)
+        return root, Tree(handle, self.field, [m.shape for m in mats])
 
     def commit_dev(self, mats) -> Tuple[np.ndarray, Tree]:
         """Commit CUDA torch tensors in place; they must outlive the returned tree."""
@@ -226,7 +226,7 @@ class CudaMerkleTreeMmcs:
         stream = C.c_void_p(torch.cuda.current_stream(mats[0].device).cuda_stream)
         N.check(N.load().zkb_mmcs_commit_dev(C.byref(self.hasher), descs, len(mats), _ptr(root),
                                              C.byref(handle), stream))
-        t = Tree(handle, self.field, [np.empty((m.shape[0], m.shape[1]), dtype=np.uint8) for m in mats])
+        t = Tree(handle, self.field, [tuple(m.shape) for m in mats])
         t._keepalive = list(mats)
         return root, t
 
@@ -243,6 +243,52 @@ class CudaMerkleTreeMmcs:
             out.append(rows[off:off + w].copy())
             off += w
         return out, [sib[i * self.digest_elems:(i + 1) * self.digest_elems].copy() for i in range(log_max)]
+
+
+# ----------------------------------------------------------------------- PCS
+class CudaTwoAdicPcs:
+    """TwoAdicFriPcs::commit for a trace matrix (Pcs at zkf-backends/src/plonky3.rs:68):
+    coset LDE by 2^log_blowup, bit-reversed rows, Poseidon2 MMCS commit.  The LDE stays
+    on the device as the tree's leaf matrix."""
+
+    def __init__(self, field: int, seed: int, log_blowup: int, width: int = 16):
+        self.mmcs = CudaMerkleTreeMmcs(field, seed, width)
+        self.field = field
+        self.log_blowup = log_blowup
+
+    def commit(self, trace: np.ndarray) -> Tuple[np.ndarray, Tree]:
+        t = np.ascontiguousarray(trace, dtype=dtype_of(self.field))
+        h, w = t.shape
+        root = np.zeros(self.mmcs.digest_elems, dtype=dtype_of(self.field))
+        handle = C.c_void_p()
+        N.check(N.load().zkb_pcs_commit(C.byref(self.mmcs.hasher), _ptr(t), h.bit_length() - 1, w,
+                                        self.log_blowup, _ptr(root), C.byref(handle)))
+        return root, Tree(handle, self.field, [(h << self.log_blowup, w)])
+
+    def commit_ptr(self, host_ptr: int, height: int, width: int, want_tree: bool = True,
+                   root: Optional[np.ndarray] = None):
+        """Host-pointer form for caller-managed (e.g. pinned) buffers."""
+        root = np.zeros(self.mmcs.digest_elems, dtype=dtype_of(self.field)) if root is None else root
+        handle = C.c_void_p()
+        N.check(N.load().zkb_pcs_commit(C.byref(self.mmcs.hasher), C.c_void_p(host_ptr),
+                                        height.bit_length() - 1, width, self.log_blowup, _ptr(root),
+                                        C.byref(handle) if want_tree else None))
+        tree = Tree(handle, self.field, [(height << self.log_blowup, width)]) \
+            if want_tree else None
+        return root, tree
+
+    def commit_dev(self, trace, want_tree: bool = True, root: Optional[np.ndarray] = None):
+        """Device form on a CUDA torch tensor (h x w), on the tensor's current stream."""
+        h, w = trace.shape
+        ptr, stream = _torch_ptr_stream(trace)
+        root = np.zeros(self.mmcs.digest_elems, dtype=dtype_of(self.field)) if root is None else root
+        handle = C.c_void_p()
+        N.check(N.load().zkb_pcs_commit_dev(C.byref(self.mmcs.hasher), ptr, h.bit_length() - 1, w,
+                                            self.log_blowup, _ptr(root),
+                                            C.byref(handle) if want_tree else None, stream))
+        tree = Tree(handle, self.field, [(h << self.log_blowup, w)]) \
+            if want_tree else None
+        return root, tree
 
 
 # --------------------------------------------------------------------------- FRI

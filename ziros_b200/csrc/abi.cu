@@ -8,6 +8,7 @@
 
 namespace zkb {
 const char *last_error();
+int measure_mul_peak(int field, double *mul_per_s);
 }
 
 using namespace zkb;
@@ -133,6 +134,24 @@ int zkb_set_device(int device) {
   clear_error();
   ZKB_CHECK_CUDA(cudaSetDevice(device));
   return ZKB_OK;
+}
+
+int zkb_measure_mul_peak(int field, double *mul_per_s) {
+  ZKB_ENTRY();
+  ZKB_TRY(check_field(field));
+  ZKB_REQUIRE(mul_per_s != nullptr, "null output");
+  return measure_mul_peak(field, mul_per_s);
+}
+
+int zkb_profile_start(void) {
+  clear_error();
+  return profile_start();
+}
+
+int zkb_profile_stop(zkb_kernel_stat *out, int cap) {
+  clear_error();
+  ZKB_REQUIRE(out != nullptr || cap == 0, "null output");
+  return profile_stop(out, cap);
 }
 
 // ------------------------------------------------------------------ Poseidon2
@@ -281,6 +300,64 @@ int zkb_mmcs_commit(const zkb_hasher *hasher, const zkb_matrix *mats, size_t n_m
   }
   ZKB_TRY(mmcs_build_dev(spec, dm, &tree->t, s));
   return tree_from(tree_out, tree, root_out, s);
+}
+
+namespace {
+int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_trace, uint32_t log_h,
+                    uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out,
+                    cudaStream_t s) {
+  ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
+  const size_t es = field_elem_bytes(spec.field);
+  const uint64_t n = 1ull << log_h, N = n << log_blowup;
+  auto tree = std::make_unique<zkb_tree>();
+  tree->t.stream = s;
+  ZKB_CHECK_CUDA(cudaGetDevice(&tree->t.device));
+  ScratchBuf staged;
+  if (h_trace) {
+    ZKB_TRY(staged.alloc(n * width * es, s));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(staged.p, h_trace, n * width * es, cudaMemcpyHostToDevice, s));
+    d_trace = staged.p;
+  }
+  void *lde = nullptr;
+  ZKB_TRY(dev_alloc(&lde, N * width * es, s));
+  tree->t.owned.push_back(lde);
+  int rc;
+  if (spec.field == FIELD_BABYBEAR)
+    rc = ntt_lde_dev<BabyBear>((const uint32_t *)d_trace, (int)log_h, width, (int)log_blowup,
+                               BabyBear::GENERATOR, true, (uint32_t *)lde, s);
+  else
+    rc = ntt_lde_dev<Goldilocks>((const uint64_t *)d_trace, (int)log_h, width, (int)log_blowup,
+                                 Goldilocks::GENERATOR, true, (uint64_t *)lde, s);
+  ZKB_TRY(rc);
+  std::vector<TreeMatrix> mats{{lde, N, width}};
+  ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));
+  return tree_from(tree_out, tree, root_out, s);
+}
+}  // namespace
+
+int zkb_pcs_commit(const zkb_hasher *hasher, const void *trace, uint32_t log_h, uint32_t width,
+                   uint32_t log_blowup, void *root_out, zkb_tree **tree_out) {
+  ZKB_ENTRY();
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(trace != nullptr && width > 0, "empty trace");
+  return pcs_commit_impl(spec, nullptr, trace, log_h, width, log_blowup, root_out, tree_out,
+                         thread_stream());
+}
+
+int zkb_pcs_commit_dev(const zkb_hasher *hasher, const void *d_trace, uint32_t log_h, uint32_t width,
+                       uint32_t log_blowup, void *root_out, zkb_tree **tree_out, void *stream) {
+  ZKB_ENTRY();
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(d_trace != nullptr && width > 0, "empty trace");
+  return pcs_commit_impl(spec, d_trace, nullptr, log_h, width, log_blowup, root_out, tree_out,
+                         resolve_stream(stream));
+}
+
+const void *zkb_tree_matrix_dev(const zkb_tree *tree, int mat) {
+  if (!tree || mat < 0 || mat >= (int)tree->t.mats.size()) return nullptr;
+  return tree->t.mats[mat].data;
 }
 
 int zkb_tree_num_layers(const zkb_tree *tree) {

@@ -90,6 +90,32 @@ struct ScratchBuf {
   }
 };
 
+// ---- kernel timing (zkb_profile_start / zkb_profile_stop) ----
+// When enabled, every launch made through ZKB_LAUNCH records a pair of CUDA events
+// on its own stream; zkb_profile_stop aggregates the durations per kernel name.
+bool profiling_enabled();
+int profile_start();
+int profile_stop(zkb_kernel_stat *out, int cap);
+int prof_record(const char *name, cudaStream_t s, int phase, void **token);
+
+struct ProfScope {
+  void *tok = nullptr;
+  cudaStream_t s;
+  ProfScope(const char *name, cudaStream_t st) : s(st) {
+    if (profiling_enabled()) prof_record(name, s, 0, &tok);
+  }
+  ~ProfScope() {
+    if (tok) prof_record(nullptr, s, 1, &tok);
+  }
+};
+
+#define ZKB_LAUNCH(name, stream, ...)              \
+  do {                                             \
+    ::zkb::ProfScope zkb_ps_((name), (stream));    \
+    __VA_ARGS__;                                   \
+    ZKB_CHECK_LAUNCH();                            \
+  } while (0)
+
 inline size_t field_elem_bytes(int field) { return field == ZKB_FIELD_BABYBEAR ? 4 : 8; }
 
 inline int ilog2_exact(uint64_t x) {

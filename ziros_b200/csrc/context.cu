@@ -1,5 +1,6 @@
 // context.cu — per-device context, per-thread streams, last-error, scratch memory.
 #include <cstdio>
+#include <cstring>
 #include <memory>
 #include <vector>
 
@@ -68,6 +69,93 @@ cudaStream_t thread_stream() {
     t_streams.per_dev[dev] = s;
   }
   return t_streams.per_dev[dev];
+}
+
+// --------------------------------------------------------------- profiling
+namespace {
+struct ProfRec {
+  const char *name;
+  int device;
+  cudaEvent_t a, b;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof;
+std::vector<std::pair<int, cudaEvent_t>> g_event_pool;
+
+cudaEvent_t take_event(int dev) {
+  for (size_t i = 0; i < g_event_pool.size(); i++)
+    if (g_event_pool[i].first == dev) {
+      cudaEvent_t e = g_event_pool[i].second;
+      g_event_pool.erase(g_event_pool.begin() + i);
+      return e;
+    }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
+bool profiling_enabled() { return g_prof_on; }
+
+int prof_record(const char *name, cudaStream_t s, int phase, void **token) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (phase == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    ProfRec r{name, dev, take_event(dev), take_event(dev)};
+    cudaEventRecord(r.a, s);
+    g_prof.push_back(r);
+    *token = (void *)(uintptr_t)g_prof.size();  // 1-based index
+  } else {
+    size_t idx = (size_t)(uintptr_t)*token - 1;
+    if (idx < g_prof.size()) cudaEventRecord(g_prof[idx].b, s);
+    *token = nullptr;
+  }
+  return ZKB_OK;
+}
+
+int profile_start() {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (auto &r : g_prof) {
+    g_event_pool.push_back({r.device, r.a});
+    g_event_pool.push_back({r.device, r.b});
+  }
+  g_prof.clear();
+  g_prof_on = true;
+  return ZKB_OK;
+}
+
+int profile_stop(zkb_kernel_stat *out, int cap) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_on = false;
+  std::vector<zkb_kernel_stat> agg;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  for (auto &r : g_prof) {
+    cudaSetDevice(r.device);
+    float ms = 0;
+    if (cudaEventSynchronize(r.b) != cudaSuccess || cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) {
+      cudaSetDevice(prev);
+      set_error("profiling events could not be read");
+      return ZKB_ERR_CUDA;
+    }
+    zkb_kernel_stat *st = nullptr;
+    for (auto &a : agg)
+      if (strncmp(a.name, r.name, sizeof a.name) == 0) st = &a;
+    if (!st) {
+      agg.push_back(zkb_kernel_stat{});
+      st = &agg.back();
+      strncpy(st->name, r.name, sizeof st->name - 1);
+    }
+    st->launches++;
+    st->total_ms += ms;
+    st->max_ms = ms > st->max_ms ? ms : st->max_ms;
+  }
+  cudaSetDevice(prev);
+  int n = (int)agg.size();
+  for (int i = 0; i < n && i < cap; i++) out[i] = agg[i];
+  return n;
 }
 
 int dev_alloc(void **p, size_t bytes, cudaStream_t s) {

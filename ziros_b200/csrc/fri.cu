@@ -64,15 +64,15 @@ int fri_fold_base_dev(const typename F::T *d_evals, size_t n_out, typename F::T 
   const T inv2 = Dom<F>::encode(inv_host<F>(2));
   const T a_enc = Dom<F>::encode(alpha);
   if (d_inv_tw) {
-    fri_fold_given_kernel<F><<<grid_for(n_out, 256), 256, 0, s>>>(d_evals, d_out, n_out, a_enc, inv2,
-                                                                  d_inv_tw);
+    ZKB_LAUNCH("fri_fold", s, fri_fold_given_kernel<F><<<grid_for(n_out, 256), 256, 0, s>>>(d_evals, d_out, n_out, a_enc, inv2,
+                                                                  d_inv_tw));
   } else {
     int log_n = ilog2_exact(n_out);
     ZKB_REQUIRE(log_n >= 0, "n_out must be a power of two when inv_twiddles is NULL");
     const T *itw;
     ZKB_TRY(get_twiddles<F>(log_n + 1, true, &itw, s));
-    fri_fold_p3_kernel<F><<<grid_for(n_out, 256), 256, 0, s>>>(d_evals, d_out, n_out, log_n, a_enc,
-                                                               inv2, itw);
+    ZKB_LAUNCH("fri_fold", s, fri_fold_p3_kernel<F><<<grid_for(n_out, 256), 256, 0, s>>>(d_evals, d_out, n_out, log_n, a_enc,
+                                                               inv2, itw));
   }
   ZKB_CHECK_LAUNCH();
   return ZKB_OK;
@@ -150,7 +150,7 @@ int fri_fold_ext4_dev(const uint32_t *d_evals, size_t n_out, const uint32_t beta
   prm.inv2_enc = BabyBear::tw_encode(inv2);
   const uint32_t *itw;
   ZKB_TRY(get_twiddles<BabyBear>(log_n + 1, true, &itw, s));
-  fri_fold_ext4_kernel<<<grid_for(n_out, 256), 256, 0, s>>>(d_evals, d_out, n_out, log_n, prm, itw);
+  ZKB_LAUNCH("fri_fold_ext4", s, fri_fold_ext4_kernel<<<grid_for(n_out, 256), 256, 0, s>>>(d_evals, d_out, n_out, log_n, prm, itw));
   ZKB_CHECK_LAUNCH();
   return ZKB_OK;
 }

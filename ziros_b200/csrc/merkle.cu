@@ -200,7 +200,7 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
   ZKB_TRY(make_list(0, ng, &ml));
   const unsigned thr = 128;
   const unsigned cap = (unsigned)ctx->sm_count * 16u;
-  hash_rows_kernel<F, W><<<grid_for(max_h, thr, cap), thr, 0, s>>>(ml, max_h, layers, p);
+  ZKB_LAUNCH("merkle_leaf_hash", s, hash_rows_kernel<F, W><<<grid_for(max_h, thr, cap), thr, 0, s>>>(ml, max_h, layers, p));
   ZKB_CHECK_LAUNCH();
   ScratchBuf inj_buf;  // digests of rows injected at one layer (sized for the largest)
 
@@ -220,12 +220,12 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
       ZKB_TRY(make_list(next_m, ni, &iml));
       inj_h = mats[ord[next_m]].height;
       if (!inj_buf.p) ZKB_TRY(inj_buf.alloc(inj_h * OUT * sizeof(T), s));
-      hash_rows_kernel<F, W><<<grid_for(inj_h, thr, cap), thr, 0, s>>>(iml, inj_h, inj_buf.as<T>(), p);
+      ZKB_LAUNCH("merkle_inject_hash", s, hash_rows_kernel<F, W><<<grid_for(inj_h, thr, cap), thr, 0, s>>>(iml, inj_h, inj_buf.as<T>(), p));
       ZKB_CHECK_LAUNCH();
       inj = inj_buf.as<T>();
     }
     next_m += ni;
-    compress_kernel<F, W><<<grid_for(half, thr, cap), thr, 0, s>>>(prev, next, half, inj, inj_h, p);
+    ZKB_LAUNCH("merkle_compress", s, compress_kernel<F, W><<<grid_for(half, thr, cap), thr, 0, s>>>(prev, next, half, inj, inj_h, p));
     ZKB_CHECK_LAUNCH();
   }
   return ZKB_OK;

@@ -63,7 +63,7 @@ static int launch_powers(typename F::T *out, uint64_t n, typename F::T base, typ
     b = F::mul_host(b, b);
   }
   pp.scale = Dom<F>::encode(scale);
-  powers_kernel<F><<<grid_for(n, 256), 256, 0, s>>>(out, n, pp);
+  ZKB_LAUNCH("table_powers", s, powers_kernel<F><<<grid_for(n, 256), 256, 0, s>>>(out, n, pp));
   ZKB_CHECK_LAUNCH();
   return ZKB_OK;
 }
@@ -258,7 +258,7 @@ static int run_passes(const typename F::T *in, typename F::T *out, int L, uint32
     }
     size_t smem = (((size_t)1 << g.k) << lc) * sizeof(T) + ((size_t)1 << (g.k - 1)) * sizeof(T);
     T scale = (pi + 1 == ks.size()) ? last_scale : (T)0;
-    ntt_pass_kernel<F><<<(unsigned)ctas, 256, smem, s>>>(src, out, g, tw, scale);
+    ZKB_LAUNCH("ntt_pass", s, ntt_pass_kernel<F><<<(unsigned)ctas, 256, smem, s>>>(src, out, g, tw, scale));
     ZKB_CHECK_LAUNCH();
     src = out;
     hi = g.lo;
@@ -309,8 +309,8 @@ int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaS
   T scale = 0;
   if (inverse) scale = Dom<F>::encode(inv_host<F>((T)(n % (uint64_t)F::P)));
   ZKB_TRY(run_passes<F>(d, tmp.as<T>(), log_h, width, 1, tw, scale, s));
-  bitrev_rows_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(tmp.as<T>(), d, log_h, width,
-                                                                   n * width);
+  ZKB_LAUNCH("bitrev_rows", s, bitrev_rows_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(tmp.as<T>(), d, log_h, width,
+                                                                   n * width));
   ZKB_CHECK_LAUNCH();
   return ZKB_OK;
 }
@@ -336,8 +336,8 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
   }
   const T *ctab;
   ZKB_TRY(get_coset_table<F>(log_h, log_b, shift, &ctab, s));
-  lde_expand_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(coef.as<T>(), d_out, log_h, log_b,
-                                                                  width, ctab);
+  ZKB_LAUNCH("lde_expand", s, lde_expand_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(coef.as<T>(), d_out, log_h, log_b,
+                                                                  width, ctab));
   ZKB_CHECK_LAUNCH();
   if (log_h > 0) {
     const T *tw;
@@ -349,7 +349,7 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
     const uint64_t total = (n << log_b) * width;
     ScratchBuf tmp;
     ZKB_TRY(tmp.alloc(total * sizeof(T), s));
-    bitrev_rows_kernel<F><<<grid_for(total, 256), 256, 0, s>>>(d_out, tmp.as<T>(), LN, width, total);
+    ZKB_LAUNCH("bitrev_rows", s, bitrev_rows_kernel<F><<<grid_for(total, 256), 256, 0, s>>>(d_out, tmp.as<T>(), LN, width, total));
     ZKB_CHECK_LAUNCH();
     ZKB_CHECK_CUDA(cudaMemcpyAsync(d_out, tmp.p, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
   }

@@ -57,7 +57,7 @@ int p2_permute_batch(typename F::T *d_states, size_t n_states, const P2Params<F,
   ZKB_TRY(current_context(&ctx));
   const unsigned threads = 128;
   unsigned grid = grid_for(n_states, threads, (unsigned)ctx->sm_count * 16u);
-  p2_batch_kernel<F, W><<<grid, threads, 0, s>>>(d_states, n_states, p);
+  ZKB_LAUNCH("p2_permute", s, p2_batch_kernel<F, W><<<grid, threads, 0, s>>>(d_states, n_states, p));
   ZKB_CHECK_LAUNCH();
   return ZKB_OK;
 }
