@@ -123,6 +123,20 @@ ZKB_API int zkb_dft_batch(int field, void *rowmajor, uint32_t log_h, uint32_t wi
 ZKB_API int zkb_dft_batch_dev(int field, void *d_rowmajor, uint32_t log_h, uint32_t width, int inverse,
                       void *stream);
 
+/* Allocation-free form of zkb_dft_batch_dev, for callers that cannot call cudaMalloc
+ * (device memory owned by another allocator, or a path that must not pay the
+ * synchronisation an allocation or free can cause).  No counterpart in the reference.
+ * Its scratch is a fixed 16 MiB device array held by the library on every GPU that
+ * loads it; it must fit the twiddle table plus a copy of the matrix:
+ * 2^log_h * elem_bytes (rounded up to 256) + 2^log_h * width * elem_bytes <= 16 MiB,
+ * else ZKB_ERR_INVALID with a message.  The first call on a device looks up the
+ * array's device address (set-up, once per device); make that first call before any
+ * stream capture.  All calls share the array and it keeps the last call's contents
+ * (nothing in it needs to start at zero); calls that overlap on the GPU race, so issue
+ * them on one stream. */
+ZKB_API int zkb_dft_batch_noalloc_dev(int field, void *d_rowmajor, uint32_t log_h, uint32_t width,
+                                      int inverse, void *stream);
+
 /* p3 coset_lde_batch(trace, log_blowup, shift) followed, when bitrev_rows=1, by
  * bit_reverse_rows — the LDE that TwoAdicFriPcs::commit hands to the MMCS
  * (zkf-backends/src/plonky3.rs:250-262 -> p3-dft 0.4.2;

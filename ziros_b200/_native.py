@@ -73,6 +73,7 @@ SIGNATURES = {
     "zkb_poseidon2_goldilocks_permute_dev": (_I, [_P, _SZ, _P, _SZ, _U32, _U32, _P]),
     "zkb_dft_batch": (_I, [_I, _P, _U32, _U32, _I]),
     "zkb_dft_batch_dev": (_I, [_I, _P, _U32, _U32, _I, _P]),
+    "zkb_dft_batch_noalloc_dev": (_I, [_I, _P, _U32, _U32, _I, _P]),
     "zkb_coset_lde_batch": (_I, [_I, _P, _U32, _U32, _U32, _U64, _I, _P]),
     "zkb_coset_lde_batch_dev": (_I, [_I, _P, _U32, _U32, _U32, _U64, _I, _P, _P]),
     "zkb_mmcs_commit": (_I, [_P, _P, _SZ, _P, _P]),

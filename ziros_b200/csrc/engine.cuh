@@ -26,6 +26,10 @@ int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaS
 template <class F>
 int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log_b,
                 typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s);
+// Natural-order DFT with caller-supplied twiddle (2^log_h) and temp (2^log_h x width) buffers.
+template <class F>
+int ntt_dft_into(typename F::T *d, int log_h, uint32_t width, bool inverse, typename F::T *tw_buf,
+                 typename F::T *tmp, cudaStream_t s);
 // Cached table of w^t (t < 2^log_n) for w = two_adic_generator(log_n)^(+-1), encoded
 // for Field::mul_tw (Montgomery form for BabyBear).
 template <class F>

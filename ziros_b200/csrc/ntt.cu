@@ -356,6 +356,28 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
   return ZKB_OK;
 }
 
+// Natural-order column DFT whose twiddle table and out-of-place temp are supplied by the
+// caller (tw_buf: 2^log_h elements, tmp: 2^log_h x width elements); the table is
+// regenerated into tw_buf on every call.  Used by the allocation-free entry point.
+template <class F>
+int ntt_dft_into(typename F::T *d, int log_h, uint32_t width, bool inverse, typename F::T *tw_buf,
+                 typename F::T *tmp, cudaStream_t s) {
+  using T = typename F::T;
+  if (width == 0 || log_h == 0) return ZKB_OK;
+  const uint64_t n = 1ull << log_h;
+  T w = two_adic_generator<F>(log_h);
+  if (inverse) w = inv_host<F>(w);
+  ZKB_TRY(launch_powers<F>(tw_buf, n, w, 1, s));
+  T scale = 0;
+  if (inverse) scale = Dom<F>::encode(inv_host<F>((T)(n % (uint64_t)F::P)));
+  ZKB_TRY(run_passes<F>(d, tmp, log_h, width, 1, tw_buf, scale, s));
+  ZKB_LAUNCH("bitrev_rows", s, bitrev_rows_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(tmp, d, log_h, width, n * width));
+  return ZKB_OK;
+}
+
+template int ntt_dft_into<BabyBear>(uint32_t *, int, uint32_t, bool, uint32_t *, uint32_t *, cudaStream_t);
+template int ntt_dft_into<Goldilocks>(uint64_t *, int, uint32_t, bool, uint64_t *, uint64_t *, cudaStream_t);
+
 template int get_twiddles<BabyBear>(int, bool, const uint32_t **, cudaStream_t);
 template int get_twiddles<Goldilocks>(int, bool, const uint64_t **, cudaStream_t);
 template int ntt_dft_dev<BabyBear>(uint32_t *, int, uint32_t, bool, cudaStream_t);
