@@ -223,6 +223,66 @@ ZKB_API int zkb_fri_fold_babybear(const uint32_t *evals, size_t n_evals, uint32_
 ZKB_API int zkb_fri_fold_babybear_ext4(const uint32_t *evals, size_t n_out, const uint32_t *beta,
                                uint32_t *out);
 
+/* FRI commit phase over the BabyBear quartic extension with seeded challenges — the
+ * prove_fri commit phase and query answers of p3-fri 0.4.2 as TwoAdicFriPcs runs them
+ * (PCS at zkf-backends/src/plonky3.rs:68, FRI parameters :597), folding with
+ * p3 fold_matrix (see zkb_fri_fold_babybear_ext4).  Round r commits the codeword
+ * (2^(log_n-r) extension elements, bit-reversed domain order) as rows of the pairs
+ * (x, -x), 8 base elements each (ExtensionMmcs flattening), then folds with beta_r.
+ * beta_r = four BabyBear draws (p3 sampler) from SmallRng(challenge_seed); query
+ * indices are next_u64() >> (64 - log_n) from SmallRng(query_seed).  Each query opens,
+ * per round, the row (index >> r) >> 1 and its sibling path. */
+typedef struct {
+  uint32_t log_n;           /* codeword length 2^log_n extension elements */
+  uint32_t log_final;       /* stop at 2^log_final elements */
+  uint64_t challenge_seed;  /* betas */
+  uint32_t num_queries;
+  uint64_t query_seed;
+} zkb_fri_params;
+typedef struct zkb_fri_proof zkb_fri_proof;
+/* Host form: `codeword` holds 2^log_n x 4 u32 (coefficients of each element). */
+ZKB_API int zkb_fri_commit_babybear_ext4(const zkb_hasher *hasher, const zkb_fri_params *params,
+                                         const uint32_t *codeword, zkb_fri_proof **proof_out);
+ZKB_API int zkb_fri_commit_babybear_ext4_dev(const zkb_hasher *hasher, const zkb_fri_params *params,
+                                             const uint32_t *d_codeword, zkb_fri_proof **proof_out,
+                                             void *stream);
+ZKB_API int zkb_fri_num_rounds(const zkb_fri_proof *proof);
+/* Per-round commitments (rounds x 8 u32) and challenges (rounds x 4 u32). */
+ZKB_API int zkb_fri_commitments(const zkb_fri_proof *proof, uint32_t *roots_out, uint32_t *betas_out);
+/* Final codeword: 2^log_final x 4 u32. */
+ZKB_API int zkb_fri_final_codeword(const zkb_fri_proof *proof, uint32_t *out);
+/* Sibling elements per query (sum over rounds of (log_n - r - 1) x 8). */
+ZKB_API int64_t zkb_fri_siblings_per_query(const zkb_fri_proof *proof);
+/* Query answers: indices (num_queries), opened rows (num_queries x rounds x 8 u32) and
+ * sibling paths (num_queries x siblings_per_query u32), round-major within a query. */
+ZKB_API int zkb_fri_query_openings(const zkb_fri_proof *proof, uint64_t *indices_out,
+                                   uint32_t *rows_out, uint32_t *siblings_out);
+ZKB_API void zkb_fri_proof_free(zkb_fri_proof *proof);
+
+/* The batched codeword of a PCS opening, without the division by (x - z): for each LDE
+ * row i, out[i] = sum_j alpha^j * lde[i][j] in the BabyBear quartic extension — the
+ * alpha-reduction TwoAdicFriPcs applies to the committed columns before FRI
+ * (p3-fri 0.4.2 open, PCS at zkf-backends/src/plonky3.rs:68).  Device pointers:
+ * `d_lde` rows x width u32, `d_out` rows x 4 u32 (16-byte aligned). */
+ZKB_API int zkb_combine_columns_babybear_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
+                                                  const uint32_t *alpha, uint32_t *d_out, void *stream);
+
+/* One commitment job of the Plonky3 PCS for a BabyBear trace, device-resident from end
+ * to end: zkb_pcs_commit (coset LDE, bit-reversed rows, MMCS), then the alpha-reduction
+ * of the committed LDE columns into one F_p^4 codeword (zkb_combine_columns_...), then
+ * the FRI commit phase and query answers on it (zkb_fri_commit_babybear_ext4;
+ * params->log_n is set to log_h + log_blowup).  This is TwoAdicFriPcs commit + open
+ * without the (x - z) quotient and the transcript (PCS at zkf-backends/src/plonky3.rs:68).
+ * Outputs: the trace root (8 u32), the tree (may be NULL) and the FRI proof (may be NULL). */
+ZKB_API int zkb_pcs_commit_fri(const zkb_hasher *hasher, const void *trace, uint32_t log_h,
+                               uint32_t width, uint32_t log_blowup, const uint32_t *alpha,
+                               const zkb_fri_params *params, void *root_out, zkb_tree **tree_out,
+                               zkb_fri_proof **fri_out);
+ZKB_API int zkb_pcs_commit_fri_dev(const zkb_hasher *hasher, const void *d_trace, uint32_t log_h,
+                                   uint32_t width, uint32_t log_blowup, const uint32_t *alpha,
+                                   const zkb_fri_params *params, void *root_out, zkb_tree **tree_out,
+                                   zkb_fri_proof **fri_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,8 @@ def lib():
             "or_two_adic_generator": (u64, [C.c_int, C.c_int]),
             "or_field_generator": (u64, [C.c_int]),
             "or_rng_fill_u64": (None, [u64, P, sz]),
+            "or_rng_fill_bb": (None, [u64, P, sz]),
+            "or_combine_columns_ext4": (None, [P, sz, sz, P, P]),
             "or_p2_round_numbers": (C.c_int, [C.c_int, C.c_int, P, P]),
             "or_p2_constants_bb": (C.c_int, [u64, C.c_int, P, sz]),
             "or_p2_constants_gl": (C.c_int, [u64, C.c_int, P, sz]),
@@ -280,3 +282,49 @@ def num_threads() -> int:
 
 def set_threads(n: int) -> None:
     lib().or_set_threads(n)
+
+
+def rng_bb(seed: int, n: int) -> np.ndarray:
+    """n BabyBear draws (p3 sampler) from SmallRng(seed)."""
+    out = np.empty(n, dtype=np.uint32)
+    lib().or_rng_fill_bb(seed, _ptr(out), n)
+    return out
+
+
+def combine_columns_ext4(lde: np.ndarray, alpha) -> np.ndarray:
+    m = np.ascontiguousarray(lde, dtype=np.uint32)
+    a = np.ascontiguousarray(alpha, dtype=np.uint32)
+    out = np.zeros((m.shape[0], 4), dtype=np.uint32)
+    lib().or_combine_columns_ext4(_ptr(m), m.shape[0], m.shape[1], _ptr(a), _ptr(out))
+    return out
+
+
+def fri_commit_ext4(codeword: np.ndarray, log_final: int, p2_seed: int, challenge_seed: int,
+                    num_queries: int, query_seed: int) -> dict:
+    """FRI commit phase with seeded challenges (p3 commit_phase/answer_query restated):
+    round r commits the codeword as rows of (x, -x) pairs flattened to 8 base elements,
+    then folds with beta_r; queries open row (index >> r) >> 1 of every round."""
+    cw = np.ascontiguousarray(codeword, dtype=np.uint32).reshape(-1, 4)
+    log_n = cw.shape[0].bit_length() - 1
+    rounds = log_n - log_final
+    h = hasher(BABYBEAR, p2_seed)
+    betas = rng_bb(challenge_seed, 4 * rounds).reshape(rounds, 4)
+    trees, leaves = [], []
+    cur = cw
+    for r in range(rounds):
+        mat = cur.reshape(-1, 8)
+        layers = mmcs_commit(h, [mat])
+        trees.append(layers)
+        leaves.append(mat)
+        cur = fri_fold_ext4(cur, betas[r])
+    idx = (rng_u64(query_seed, num_queries) >> np.uint64(64 - log_n)).astype(np.uint64)
+    queries = []
+    for q in idx:
+        per_round = []
+        for r in range(rounds):
+            pair = (int(q) >> r) >> 1
+            rows, proof = mmcs_open(trees[r], [leaves[r]], pair)
+            per_round.append((rows[0], proof))
+        queries.append(per_round)
+    return {"roots": np.array([t[-1][0] for t in trees]), "betas": betas, "final": cur,
+            "indices": idx, "queries": queries}

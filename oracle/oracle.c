@@ -156,6 +156,12 @@ uint32_t or_sample_bb(or_rng *r) {
   }
 }
 
+void or_rng_fill_bb(uint64_t seed, uint32_t *out, size_t n) {
+  or_rng r;
+  or_rng_seed(&r, seed);
+  for (size_t i = 0; i < n; i++) out[i] = or_sample_bb(&r);
+}
+
 void or_rng_fill_u64(uint64_t seed, uint64_t *out, size_t n) {
   or_rng r;
   or_rng_seed(&r, seed);
@@ -726,6 +732,28 @@ void or_fri_fold_ext4(const uint32_t *evals, size_t n_out, const uint32_t beta[4
     for (int k = 0; k < 4; k++) out[4 * i + k] = or_bb_add(a[k], b[k]);
   }
   free(pows);
+}
+
+/* out[i] = sum_j alpha^j * lde[i][j] in BabyBear^4: the alpha-reduction of committed
+ * columns into one extension codeword (p3-fri 0.4.2 open, without the (x - z) quotient). */
+void or_combine_columns_ext4(const uint32_t *lde, size_t rows, size_t width, const uint32_t alpha[4],
+                             uint32_t *out) {
+  uint32_t *pw = (uint32_t *)malloc(16 * (width ? width : 1));
+  uint32_t cur[4] = {1, 0, 0, 0};
+  for (size_t j = 0; j < width; j++) {
+    memcpy(pw + 4 * j, cur, 16);
+    uint32_t nx[4];
+    or_bb4_mul(cur, alpha, nx);
+    memcpy(cur, nx, 16);
+  }
+#pragma omp parallel for schedule(static)
+  for (size_t r = 0; r < rows; r++) {
+    uint32_t acc[4] = {0, 0, 0, 0};
+    for (size_t j = 0; j < width; j++)
+      for (int k = 0; k < 4; k++) acc[k] = or_bb_add(acc[k], or_bb_mul(lde[r * width + j], pw[4 * j + k]));
+    memcpy(out + 4 * r, acc, 16);
+  }
+  free(pw);
 }
 
 int or_num_threads(void) {

@@ -56,6 +56,7 @@ uint64_t or_sample_gl(or_rng *r);
 uint32_t or_sample_bb(or_rng *r);
 /* Fill `out` with `n` draws; returns final rng state in *r. */
 void or_rng_fill_u64(uint64_t seed, uint64_t *out, size_t n);
+void or_rng_fill_bb(uint64_t seed, uint32_t *out, size_t n);
 
 /* ---- Poseidon2 ---- */
 int or_p2_round_numbers(int field, int width, int *rounds_f, int *rounds_p);
@@ -121,6 +122,8 @@ void or_fri_fold_ext4(const uint32_t *evals, size_t n_out, const uint32_t beta[4
  * inv_tw[i] = g_inv^{rev(i)} / 2, g = two_adic_generator(log2(n_out)+1). */
 void or_fri_inv_twiddles(int field, size_t n_out, void *out);
 void or_bb4_mul(const uint32_t *a, const uint32_t *b, uint32_t *out);
+void or_combine_columns_ext4(const uint32_t *lde, size_t rows, size_t width, const uint32_t alpha[4],
+                             uint32_t *out);
 
 /* ---- timing helper for the CPU baseline ---- */
 int or_num_threads(void);

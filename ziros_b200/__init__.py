@@ -10,6 +10,9 @@ from .accel import (  # noqa: F401
     GOLDILOCKS,
     CudaDft,
     CudaFri,
+    CudaFriProver,
+    FriProof,
+    combine_columns_dev,
     CudaMerkleTreeMmcs,
     CudaPoseidon2,
     CudaTwoAdicPcs,

@@ -51,6 +51,11 @@ class Hasher(C.Structure):
     _fields_ = [("field", C.c_int), ("width", C.c_uint32), ("seed", C.c_uint64)]
 
 
+class FriParams(C.Structure):
+    _fields_ = [("log_n", C.c_uint32), ("log_final", C.c_uint32), ("challenge_seed", C.c_uint64),
+                ("num_queries", C.c_uint32), ("query_seed", C.c_uint64)]
+
+
 # Every symbol of include/zkb200.h with its ctypes signature.
 _P = C.c_void_p
 _SZ = C.c_size_t
@@ -90,6 +95,17 @@ SIGNATURES = {
     "zkb_fri_fold_goldilocks": (_I, [_P, _SZ, _U64, _P, _P]),
     "zkb_fri_fold_babybear": (_I, [_P, _SZ, _U32, _P, _P]),
     "zkb_fri_fold_babybear_ext4": (_I, [_P, _SZ, _P, _P]),
+    "zkb_fri_commit_babybear_ext4": (_I, [_P, _P, _P, _P]),
+    "zkb_fri_commit_babybear_ext4_dev": (_I, [_P, _P, _P, _P, _P]),
+    "zkb_fri_num_rounds": (_I, [_P]),
+    "zkb_fri_commitments": (_I, [_P, _P, _P]),
+    "zkb_fri_final_codeword": (_I, [_P, _P]),
+    "zkb_fri_siblings_per_query": (C.c_int64, [_P]),
+    "zkb_fri_query_openings": (_I, [_P, _P, _P, _P]),
+    "zkb_fri_proof_free": (None, [_P]),
+    "zkb_combine_columns_babybear_ext4_dev": (_I, [_P, _U64, _U32, _P, _P, _P]),
+    "zkb_pcs_commit_fri": (_I, [_P, _P, _U32, _U32, _U32, _P, _P, _P, _P, _P]),
+    "zkb_pcs_commit_fri_dev": (_I, [_P, _P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

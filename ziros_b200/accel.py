@@ -291,6 +291,44 @@ class CudaTwoAdicPcs:
         return root, tree
 
 
+    # -- commit + FRI job (BabyBear) ------------------------------------------------
+    def _fri_call(self, dev: bool, ptr, stream, h: int, w: int, alpha, log_final: int, num_queries: int,
+                  challenge_seed: int, query_seed: int, want_tree: bool, root):
+        a = np.ascontiguousarray(alpha, dtype=np.uint32)
+        log_n = (h.bit_length() - 1) + self.log_blowup
+        prm = N.FriParams(log_n, log_final, challenge_seed, num_queries, query_seed)
+        root = np.zeros(8, np.uint32) if root is None else root
+        th, fh = C.c_void_p(), C.c_void_p()
+        args = [C.byref(self.mmcs.hasher), ptr, h.bit_length() - 1, w, self.log_blowup, _ptr(a), C.byref(prm),
+                _ptr(root), C.byref(th) if want_tree else None, C.byref(fh)]
+        lib = N.load()
+        if dev:
+            N.check(lib.zkb_pcs_commit_fri_dev(*args, stream))
+        else:
+            N.check(lib.zkb_pcs_commit_fri(*args))
+        tree = Tree(th, self.field, [(h << self.log_blowup, w)]) if want_tree else None
+        return root, tree, FriProof(fh, prm)
+
+    def commit_fri(self, trace: np.ndarray, alpha, log_final: int, num_queries: int, challenge_seed: int,
+                   query_seed: int, want_tree: bool = True):
+        """Commit the trace, reduce its LDE columns with alpha, run the FRI commit phase:
+        returns (root, tree, FriProof)."""
+        t = np.ascontiguousarray(trace, dtype=np.uint32)
+        return self._fri_call(False, _ptr(t), None, t.shape[0], t.shape[1], alpha, log_final, num_queries,
+                              challenge_seed, query_seed, want_tree, None)
+
+    def commit_fri_ptr(self, host_ptr: int, height: int, width: int, alpha, log_final: int, num_queries: int,
+                       challenge_seed: int, query_seed: int, want_tree: bool = False, root=None):
+        return self._fri_call(False, C.c_void_p(host_ptr), None, height, width, alpha, log_final, num_queries,
+                              challenge_seed, query_seed, want_tree, root)
+
+    def commit_fri_dev(self, trace, alpha, log_final: int, num_queries: int, challenge_seed: int,
+                       query_seed: int, want_tree: bool = False, root=None):
+        ptr, stream = _torch_ptr_stream(trace)
+        return self._fri_call(True, ptr, stream, trace.shape[0], trace.shape[1], alpha, log_final, num_queries,
+                              challenge_seed, query_seed, want_tree, root)
+
+
 # --------------------------------------------------------------------------- FRI
 class CudaFri:
     """FRI folding (MetalFri / FriAccelerator)."""
@@ -330,3 +368,82 @@ class CudaFri:
         out = np.zeros((e.shape[0] // 2, 4), dtype=np.uint32)
         N.check(N.load().zkb_fri_fold_babybear_ext4(_ptr(e), out.shape[0], _ptr(b), _ptr(out)))
         return out
+
+
+class FriProof:
+    """Result of the FRI commit phase: per-round roots and betas, final codeword and
+    query openings (all on the host)."""
+
+    def __init__(self, handle: C.c_void_p, params: "N.FriParams"):
+        lib = N.load()
+        self._h = handle
+        self.log_n, self.log_final = params.log_n, params.log_final
+        self.rounds = lib.zkb_fri_num_rounds(handle)
+        self.roots = np.zeros((self.rounds, 8), np.uint32)
+        self.betas = np.zeros((self.rounds, 4), np.uint32)
+        N.check(lib.zkb_fri_commitments(handle, _ptr(self.roots), _ptr(self.betas)))
+        self.final = np.zeros((1 << self.log_final, 4), np.uint32)
+        N.check(lib.zkb_fri_final_codeword(handle, _ptr(self.final)))
+        nq = params.num_queries
+        spq = lib.zkb_fri_siblings_per_query(handle)
+        self.query_indices = np.zeros(nq, np.uint64)
+        self.query_rows = np.zeros((nq, self.rounds, 8), np.uint32)
+        self.query_siblings = np.zeros((nq, max(spq, 0)), np.uint32)
+        if nq:
+            N.check(lib.zkb_fri_query_openings(handle, _ptr(self.query_indices), _ptr(self.query_rows),
+                                               _ptr(self.query_siblings)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.load().zkb_fri_proof_free(h)
+            self._h = None
+
+    def siblings(self, q: int, r: int) -> np.ndarray:
+        """Sibling digests of query q in round r: (log_n - r - 1, 8)."""
+        off = sum(self.log_n - k - 1 for k in range(r)) * 8
+        depth = self.log_n - r - 1
+        return self.query_siblings[q, off:off + depth * 8].reshape(depth, 8)
+
+
+class CudaFriProver:
+    """FRI commit phase over BabyBear^4 with seeded challenges (p3 prove_fri's commit
+    phase and query answers, as TwoAdicFriPcs runs them)."""
+
+    def __init__(self, seed: int, log_final: int, num_queries: int, challenge_seed: int,
+                 query_seed: int):
+        N.load()
+        self.hasher = N.Hasher(BABYBEAR, 16, seed)
+        self.log_final = log_final
+        self.num_queries = num_queries
+        self.challenge_seed = challenge_seed
+        self.query_seed = query_seed
+
+    def _params(self, log_n: int) -> "N.FriParams":
+        return N.FriParams(log_n, self.log_final, self.challenge_seed, self.num_queries, self.query_seed)
+
+    def commit(self, codeword: np.ndarray) -> FriProof:
+        cw = np.ascontiguousarray(codeword, dtype=np.uint32).reshape(-1, 4)
+        log_n = cw.shape[0].bit_length() - 1
+        prm = self._params(log_n)
+        h = C.c_void_p()
+        N.check(N.load().zkb_fri_commit_babybear_ext4(C.byref(self.hasher), C.byref(prm), _ptr(cw), C.byref(h)))
+        return FriProof(h, prm)
+
+    def commit_dev(self, codeword) -> FriProof:
+        """codeword: CUDA tensor of 2^log_n x 4 int32 (extension coefficients)."""
+        log_n = codeword.shape[0].bit_length() - 1
+        prm = self._params(log_n)
+        ptr, stream = _torch_ptr_stream(codeword)
+        h = C.c_void_p()
+        N.check(N.load().zkb_fri_commit_babybear_ext4_dev(C.byref(self.hasher), C.byref(prm), ptr,
+                                                          C.byref(h), stream))
+        return FriProof(h, prm)
+
+
+def combine_columns_dev(lde, alpha, out) -> None:
+    """out[i] = sum_j alpha^j lde[i][j] over BabyBear^4 (CUDA tensors: rows x w, rows x 4)."""
+    a = np.ascontiguousarray(alpha, dtype=np.uint32)
+    lp, stream = _torch_ptr_stream(lde)
+    op, _ = _torch_ptr_stream(out)
+    N.check(N.load().zkb_combine_columns_babybear_ext4_dev(lp, lde.shape[0], lde.shape[1], _ptr(a), op, stream))

@@ -17,6 +17,10 @@ struct zkb_tree {
   DeviceTree t;
 };
 
+struct zkb_fri_proof {
+  FriProof f;
+};
+
 namespace {
 
 // Declines (reference fallback semantics) when the process has no usable device.
@@ -305,7 +309,8 @@ int zkb_mmcs_commit(const zkb_hasher *hasher, const zkb_matrix *mats, size_t n_m
 namespace {
 int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_trace, uint32_t log_h,
                     uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out,
-                    cudaStream_t s) {
+                    cudaStream_t s, const uint32_t *alpha = nullptr, const zkb_fri_params *fri = nullptr,
+                    zkb_fri_proof **fri_out = nullptr) {
   ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
   const size_t es = field_elem_bytes(spec.field);
   const uint64_t n = 1ull << log_h, N = n << log_blowup;
@@ -331,6 +336,20 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
   ZKB_TRY(rc);
   std::vector<TreeMatrix> mats{{lde, N, width}};
   ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));
+  if (fri) {
+    // alpha-reduction of the committed columns, then the FRI commit phase on it
+    const int log_n = (int)(log_h + log_blowup);
+    void *cw = nullptr;
+    ZKB_TRY(dev_alloc(&cw, N * 16, s));
+    auto pf = std::make_unique<zkb_fri_proof>();
+    pf->f.owned.push_back(cw);
+    pf->f.stream = s;
+    ZKB_CHECK_CUDA(cudaGetDevice(&pf->f.device));
+    ZKB_TRY(combine_columns_ext4_dev((const uint32_t *)lde, N, width, alpha, (uint32_t *)cw, s));
+    ZKB_TRY(fri_commit_ext4_dev(spec, (const uint32_t *)cw, log_n, (int)fri->log_final,
+                                fri->challenge_seed, (int)fri->num_queries, fri->query_seed, &pf->f, s));
+    if (fri_out) *fri_out = pf.release();
+  }
   return tree_from(tree_out, tree, root_out, s);
 }
 }  // namespace
@@ -353,6 +372,30 @@ int zkb_pcs_commit_dev(const zkb_hasher *hasher, const void *d_trace, uint32_t l
   ZKB_REQUIRE(d_trace != nullptr && width > 0, "empty trace");
   return pcs_commit_impl(spec, d_trace, nullptr, log_h, width, log_blowup, root_out, tree_out,
                          resolve_stream(stream));
+}
+
+int zkb_pcs_commit_fri(const zkb_hasher *hasher, const void *trace, uint32_t log_h, uint32_t width,
+                       uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *params,
+                       void *root_out, zkb_tree **tree_out, zkb_fri_proof **fri_out) {
+  ZKB_ENTRY();
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(spec.field == FIELD_BABYBEAR, "the FRI job runs over the BabyBear quartic extension");
+  ZKB_REQUIRE(trace != nullptr && width > 0 && alpha != nullptr && params != nullptr, "bad arguments");
+  return pcs_commit_impl(spec, nullptr, trace, log_h, width, log_blowup, root_out, tree_out,
+                         thread_stream(), alpha, params, fri_out);
+}
+
+int zkb_pcs_commit_fri_dev(const zkb_hasher *hasher, const void *d_trace, uint32_t log_h, uint32_t width,
+                           uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *params,
+                           void *root_out, zkb_tree **tree_out, zkb_fri_proof **fri_out, void *stream) {
+  ZKB_ENTRY();
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(spec.field == FIELD_BABYBEAR, "the FRI job runs over the BabyBear quartic extension");
+  ZKB_REQUIRE(d_trace != nullptr && width > 0 && alpha != nullptr && params != nullptr, "bad arguments");
+  return pcs_commit_impl(spec, d_trace, nullptr, log_h, width, log_blowup, root_out, tree_out,
+                         resolve_stream(stream), alpha, params, fri_out);
 }
 
 const void *zkb_tree_matrix_dev(const zkb_tree *tree, int mat) {
@@ -459,6 +502,83 @@ int zkb_fri_fold_babybear_ext4(const uint32_t *evals, size_t n_out, const uint32
   ZKB_TRY(dout.alloc(n_out * 4 * sizeof(uint32_t), s));
   ZKB_TRY(fri_fold_ext4_dev(de.as<uint32_t>(), n_out, beta, dout.as<uint32_t>(), s));
   return to_host(out, dout.p, n_out * 4 * sizeof(uint32_t), s);
+}
+
+// ------------------------------------------------------------- FRI commit phase
+namespace {
+int fri_commit_impl(const zkb_hasher *hasher, const zkb_fri_params *prm, const uint32_t *d_cw,
+                    zkb_fri_proof **out, cudaStream_t s) {
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(prm != nullptr && out != nullptr, "null arguments");
+  auto pf = std::make_unique<zkb_fri_proof>();
+  ZKB_TRY(fri_commit_ext4_dev(spec, d_cw, (int)prm->log_n, (int)prm->log_final, prm->challenge_seed,
+                              (int)prm->num_queries, prm->query_seed, &pf->f, s));
+  *out = pf.release();
+  return ZKB_OK;
+}
+}  // namespace
+
+int zkb_fri_commit_babybear_ext4_dev(const zkb_hasher *hasher, const zkb_fri_params *params,
+                                     const uint32_t *d_codeword, zkb_fri_proof **proof_out, void *stream) {
+  ZKB_ENTRY();
+  ZKB_REQUIRE(d_codeword != nullptr, "null codeword");
+  return fri_commit_impl(hasher, params, d_codeword, proof_out, resolve_stream(stream));
+}
+
+int zkb_fri_commit_babybear_ext4(const zkb_hasher *hasher, const zkb_fri_params *params,
+                                 const uint32_t *codeword, zkb_fri_proof **proof_out) {
+  ZKB_ENTRY();
+  ZKB_REQUIRE(params != nullptr && codeword != nullptr && params->log_n < 31, "bad arguments");
+  cudaStream_t s = thread_stream();
+  ScratchBuf d;
+  ZKB_TRY(to_device(d, codeword, (16ull << params->log_n), s));
+  return fri_commit_impl(hasher, params, d.as<uint32_t>(), proof_out, s);
+}
+
+int zkb_fri_num_rounds(const zkb_fri_proof *p) {
+  if (!p) return ZKB_ERR_INVALID;
+  return (int)p->f.trees.size();
+}
+
+int zkb_fri_commitments(const zkb_fri_proof *p, uint32_t *roots_out, uint32_t *betas_out) {
+  clear_error();
+  ZKB_REQUIRE(p != nullptr, "null proof");
+  if (roots_out) std::memcpy(roots_out, p->f.roots.data(), p->f.roots.size() * 4);
+  if (betas_out)
+    for (size_t r = 0; r < p->f.betas.size(); r++) std::memcpy(betas_out + 4 * r, p->f.betas[r].data(), 16);
+  return ZKB_OK;
+}
+
+int zkb_fri_final_codeword(const zkb_fri_proof *p, uint32_t *out) {
+  clear_error();
+  ZKB_REQUIRE(p != nullptr && out != nullptr, "null arguments");
+  std::memcpy(out, p->f.final_cw.data(), p->f.final_cw.size() * 4);
+  return ZKB_OK;
+}
+
+int64_t zkb_fri_siblings_per_query(const zkb_fri_proof *p) {
+  if (!p) return ZKB_ERR_INVALID;
+  return (int64_t)p->f.sib_per_query;
+}
+
+int zkb_fri_query_openings(const zkb_fri_proof *p, uint64_t *indices_out, uint32_t *rows_out,
+                           uint32_t *siblings_out) {
+  clear_error();
+  ZKB_REQUIRE(p != nullptr, "null proof");
+  if (indices_out) std::memcpy(indices_out, p->f.query_idx.data(), p->f.query_idx.size() * 8);
+  if (rows_out) std::memcpy(rows_out, p->f.query_rows.data(), p->f.query_rows.size() * 4);
+  if (siblings_out) std::memcpy(siblings_out, p->f.query_sibs.data(), p->f.query_sibs.size() * 4);
+  return ZKB_OK;
+}
+
+void zkb_fri_proof_free(zkb_fri_proof *p) { delete p; }
+
+int zkb_combine_columns_babybear_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
+                                          const uint32_t *alpha, uint32_t *d_out, void *stream) {
+  ZKB_ENTRY();
+  ZKB_REQUIRE(d_lde != nullptr && d_out != nullptr && alpha != nullptr, "null arguments");
+  return combine_columns_ext4_dev(d_lde, rows, width, alpha, d_out, resolve_stream(stream));
 }
 
 }  // extern "C"

@@ -1,5 +1,7 @@
 // engine.cuh — internal host-side interfaces between the CUDA modules.
 #pragma once
+#include <array>
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
@@ -66,5 +68,27 @@ int fri_fold_base_dev(const typename F::T *d_evals, size_t n_out, typename F::T 
                       const typename F::T *d_inv_tw, typename F::T *d_out, cudaStream_t s);
 int fri_fold_ext4_dev(const uint32_t *d_evals, size_t n_out, const uint32_t beta[4],
                       uint32_t *d_out, cudaStream_t s);
+
+// FRI commit phase over BabyBear^4 (seeded challenges) and its query openings.
+struct FriProof {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int log_n = 0, log_final = 0;
+  std::vector<std::unique_ptr<DeviceTree>> trees;  // one per round
+  std::vector<void *> owned;                       // folded codewords (leaves of rounds >= 1)
+  std::vector<std::array<uint32_t, 4>> betas;
+  std::vector<uint32_t> final_cw;                  // 2^log_final x 4, host
+  std::vector<uint32_t> roots;                     // rounds x 8, host
+  std::vector<uint64_t> query_idx;
+  std::vector<uint32_t> query_rows;                // queries x rounds x 8
+  std::vector<uint32_t> query_sibs;                // queries x sib_per_query
+  uint64_t sib_per_query = 0;
+  ~FriProof();
+};
+int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
+                             const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s);
+int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int log_n, int log_final,
+                        uint64_t challenge_seed, int num_queries, uint64_t query_seed,
+                        FriProof *pf, cudaStream_t s);
 
 }  // namespace zkb

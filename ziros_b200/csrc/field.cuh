@@ -29,31 +29,31 @@ struct BabyBear {
   static constexpr int TWO_ADICITY = 27;
   static constexpr uint32_t GENERATOR = 31;
 
-  __host__ __device__ __forceinline__ static uint32_t add(uint32_t a, uint32_t b) {
-    uint32_t s = a + b;
-    uint32_t t = s - P;
-    return s < P ? s : t;
+  static constexpr uint32_t NPINV = 0x77ffffffu;  // -p^-1 mod 2^32
+
+  // [0, 2p) -> [0, p): the wrapped difference is larger than x exactly when x < p.
+  __host__ __device__ __forceinline__ static uint32_t red(uint32_t x) {
+    uint32_t y = x - P;
+    return x < y ? x : y;
   }
+  __host__ __device__ __forceinline__ static uint32_t add(uint32_t a, uint32_t b) { return red(a + b); }
   __host__ __device__ __forceinline__ static uint32_t sub(uint32_t a, uint32_t b) {
-    uint32_t d = a - b;
-    return a >= b ? d : d + P;
+    uint32_t d = a - b, e = d + P;
+    return d < e ? d : e;
   }
   __host__ __device__ __forceinline__ static uint32_t neg(uint32_t a) { return a ? P - a : 0; }
-  // Montgomery product a*b*2^-32 mod p for a*b < p*2^32 (both < p suffices).
-  __host__ __device__ __forceinline__ static uint32_t mont(uint32_t a, uint32_t b) {
-#ifdef __CUDA_ARCH__
-    uint32_t lo = a * b;
-    uint32_t hi = __umulhi(a, b);
-    uint32_t m = lo * PINV;
-    uint32_t mp = __umulhi(m, P);
-#else
+  // Montgomery product a*b*2^-32 in [0, 2p), for a*b < p*2^32 (one operand < 2p and the
+  // other < p suffices): t = a*b, m = t*(-p^-1) mod 2^32, (t + m*p) / 2^32.  The 64-bit
+  // multiply-adds map onto wide integer multiply-adds.
+  __host__ __device__ __forceinline__ static uint32_t mont_lazy(uint32_t a, uint32_t b) {
     uint64_t t = (uint64_t)a * b;
-    uint32_t lo = (uint32_t)t, hi = (uint32_t)(t >> 32);
-    uint32_t m = lo * PINV;
-    uint32_t mp = (uint32_t)(((uint64_t)m * P) >> 32);
-#endif
-    uint32_t r = hi - mp;
-    return hi < mp ? r + P : r;
+    uint32_t m = (uint32_t)t * NPINV;
+    uint64_t u = t + (uint64_t)m * P;
+    return (uint32_t)(u >> 32);
+  }
+  // Fully reduced Montgomery product (both operands < p).
+  __host__ __device__ __forceinline__ static uint32_t mont(uint32_t a, uint32_t b) {
+    return red(mont_lazy(a, b));
   }
   __host__ __device__ __forceinline__ static uint32_t to_mont(uint32_t a) { return mont(a, R2); }
   __host__ __device__ __forceinline__ static uint32_t from_mont(uint32_t a) { return mont(a, 1); }

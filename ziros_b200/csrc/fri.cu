@@ -7,6 +7,9 @@
 // BinomialExtensionField<BabyBear, 4> (x^4 = 11):
 //   out[i] = (r0 + r1)/2 + (beta/2) * g^-rev(i) * (r0 - r1),  g = w_{2 n_out},
 // the rows (r0, r1) being the values at +x and -x of the bit-reversed domain.
+#include <array>
+#include <memory>
+
 #include "common.cuh"
 #include "engine.cuh"
 #include "field.cuh"
@@ -159,5 +162,200 @@ template int fri_fold_base_dev<BabyBear>(const uint32_t *, size_t, uint32_t, con
                                          uint32_t *, cudaStream_t);
 template int fri_fold_base_dev<Goldilocks>(const uint64_t *, size_t, uint64_t, const uint64_t *,
                                            uint64_t *, cudaStream_t);
+
+}  // namespace zkb
+
+// ============================================================================
+// FRI commit phase over the BabyBear quartic extension, with seeded challenges.
+//
+// Round r commits the current codeword (2^(log_n - r) extension elements in the
+// bit-reversed domain order) as a matrix of 2^(log_n - r - 1) rows x 8 base
+// elements — each row the pair (x, -x) flattened coefficient-wise, which is how
+// ExtensionMmcs hands an extension matrix of width 2 to the base-field MMCS — then
+// folds by 2 with beta_r (p3 commit_phase, minus the transcript: beta_r and the query
+// indices come from SmallRng seeds).  Queries open, for each round, the row holding
+// the pair of the queried index (index >> (r + 1)) and its sibling path, as p3's
+// answer_query does with open_batch.
+// ============================================================================
+namespace zkb {
+
+struct FriRoundDesc {
+  const uint32_t *leaves;    // 2^(depth) rows x 8 u32
+  const uint32_t *layers;    // digest layers of this round's tree (8 u32 per digest)
+  uint64_t layer_off[40];    // in digests
+  int depth;                 // log2(rows)
+};
+
+// One thread per (query, round): copies the opened row and the depth sibling digests.
+__global__ void fri_gather_kernel(const FriRoundDesc *__restrict__ rounds, int n_rounds,
+                                  const uint64_t *__restrict__ idx, int n_queries,
+                                  uint32_t *__restrict__ rows_out, uint32_t *__restrict__ sib_out,
+                                  const uint64_t *__restrict__ sib_off) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_queries * n_rounds) return;
+  const int q = t / n_rounds, r = t % n_rounds;
+  const FriRoundDesc &d = rounds[r];
+  const uint64_t pair = (idx[q] >> r) >> 1;
+  uint32_t *ro = rows_out + ((uint64_t)q * n_rounds + r) * 8;
+#pragma unroll
+  for (int k = 0; k < 8; k++) ro[k] = d.leaves[pair * 8 + k];
+  uint32_t *so = sib_out + (uint64_t)q * sib_off[n_rounds] + sib_off[r];
+  for (int l = 0; l < d.depth; l++) {
+    const uint64_t j = (pair >> l) ^ 1ull;
+    const uint32_t *dg = d.layers + (d.layer_off[l] + j) * 8;
+#pragma unroll
+    for (int k = 0; k < 8; k++) so[l * 8 + k] = dg[k];
+  }
+}
+
+FriProof::~FriProof() {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  trees.clear();
+  for (void *p : owned) cudaFreeAsync(p, stream);
+  cudaSetDevice(prev);
+}
+
+int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int log_n, int log_final,
+                        uint64_t challenge_seed, int num_queries, uint64_t query_seed,
+                        FriProof *pf, cudaStream_t s) {
+  ZKB_REQUIRE(spec.field == FIELD_BABYBEAR && spec.width == 16,
+              "the extension FRI commits with the BabyBear width-16 hasher");
+  ZKB_REQUIRE(log_final >= 0 && log_final < log_n && log_n <= 27,
+              "need 0 <= log_final < log_n <= 27 (got %d, %d)", log_final, log_n);
+  ZKB_REQUIRE(num_queries >= 0 && num_queries <= 4096, "num_queries out of range");
+  ZKB_REQUIRE(((uintptr_t)d_codeword & 15) == 0, "codeword must be 16-byte aligned");
+  ZKB_CHECK_CUDA(cudaGetDevice(&pf->device));
+  pf->stream = s;
+  pf->log_n = log_n;
+  pf->log_final = log_final;
+  const int rounds = log_n - log_final;
+  SmallRng rng(challenge_seed);
+  const uint32_t *cur = d_codeword;
+  uint64_t len = 1ull << log_n;
+  for (int r = 0; r < rounds; r++) {
+    auto tree = std::make_unique<DeviceTree>();
+    std::vector<TreeMatrix> m{{cur, len / 2, 8}};
+    ZKB_TRY(mmcs_build_dev(spec, m, tree.get(), s));
+    std::array<uint32_t, 4> beta;
+    for (auto &b : beta) b = sample_babybear(rng);
+    pf->betas.push_back(beta);
+    void *next = nullptr;
+    ZKB_TRY(dev_alloc(&next, (len / 2) * 16, s));
+    pf->owned.push_back(next);
+    ZKB_TRY(fri_fold_ext4_dev(cur, len / 2, beta.data(), (uint32_t *)next, s));
+    pf->trees.push_back(std::move(tree));
+    cur = (const uint32_t *)next;
+    len /= 2;
+  }
+  // final codeword and per-round roots to the host
+  pf->final_cw.resize(len * 4);
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->final_cw.data(), cur, len * 16, cudaMemcpyDeviceToHost, s));
+  pf->roots.resize((size_t)rounds * 8);
+  for (int r = 0; r < rounds; r++) {
+    const DeviceTree &t = *pf->trees[r];
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->roots.data() + (size_t)r * 8,
+                                   (const uint32_t *)t.d_layers + t.layer_off.back() * 8, 32,
+                                   cudaMemcpyDeviceToHost, s));
+  }
+  // queries
+  SmallRng qr(query_seed);
+  pf->query_idx.resize(num_queries);
+  for (auto &q : pf->query_idx) q = qr.next_u64() >> (64 - log_n);
+  std::vector<FriRoundDesc> descs(rounds);
+  std::vector<uint64_t> sib_off(rounds + 1, 0);
+  for (int r = 0; r < rounds; r++) {
+    const DeviceTree &t = *pf->trees[r];
+    FriRoundDesc &d = descs[r];
+    d.leaves = (const uint32_t *)t.mats[0].data;
+    d.layers = (const uint32_t *)t.d_layers;
+    d.depth = log_n - r - 1;
+    ZKB_REQUIRE(d.depth < 40 && (size_t)d.depth < t.layer_off.size(), "internal: FRI tree depth");
+    for (int l = 0; l < d.depth; l++) d.layer_off[l] = t.layer_off[l];
+    sib_off[r + 1] = sib_off[r] + (uint64_t)d.depth * 8;
+  }
+  pf->sib_per_query = sib_off[rounds];
+  pf->query_rows.resize((size_t)num_queries * rounds * 8);
+  pf->query_sibs.resize((size_t)num_queries * pf->sib_per_query);
+  if (num_queries > 0 && rounds > 0) {
+    ScratchBuf d_desc, d_idx, d_off, d_rows, d_sibs;
+    ZKB_TRY(d_desc.alloc(descs.size() * sizeof(FriRoundDesc), s));
+    ZKB_TRY(d_idx.alloc(num_queries * 8, s));
+    ZKB_TRY(d_off.alloc(sib_off.size() * 8, s));
+    ZKB_TRY(d_rows.alloc(pf->query_rows.size() * 4, s));
+    ZKB_TRY(d_sibs.alloc(pf->query_sibs.size() * 4, s));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(d_desc.p, descs.data(), descs.size() * sizeof(FriRoundDesc),
+                                   cudaMemcpyHostToDevice, s));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(d_idx.p, pf->query_idx.data(), num_queries * 8, cudaMemcpyHostToDevice, s));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(d_off.p, sib_off.data(), sib_off.size() * 8, cudaMemcpyHostToDevice, s));
+    const int tasks = num_queries * rounds;
+    ZKB_LAUNCH("fri_query_gather", s, fri_gather_kernel<<<(tasks + 127) / 128, 128, 0, s>>>(d_desc.as<FriRoundDesc>(), rounds, d_idx.as<uint64_t>(), num_queries, d_rows.as<uint32_t>(), d_sibs.as<uint32_t>(), d_off.as<uint64_t>()));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->query_rows.data(), d_rows.p, pf->query_rows.size() * 4,
+                                   cudaMemcpyDeviceToHost, s));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->query_sibs.data(), d_sibs.p, pf->query_sibs.size() * 4,
+                                   cudaMemcpyDeviceToHost, s));
+  }
+  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  return ZKB_OK;
+}
+
+}  // namespace zkb
+
+namespace zkb {
+
+// out[i] = sum_j alpha^j * lde[i][j] over BabyBear^4.  alpha powers are Montgomery-encoded
+// coefficientwise (a base x extension product is four Montgomery products); the four
+// running sums stay unreduced in 64 bits and are reduced once per row.
+__global__ void __launch_bounds__(256)
+    combine_columns_kernel(const uint32_t *__restrict__ lde, uint64_t rows, uint32_t width,
+                           const uint4 *__restrict__ apow, uint4 *__restrict__ out) {
+  using B = BabyBear;
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t *row = lde + r * width;
+    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (uint32_t j = 0; j < width; j++) {
+      const uint32_t v = row[j];
+      const uint4 w = apow[j];
+      a0 += B::mont_lazy(v, w.x);
+      a1 += B::mont_lazy(v, w.y);
+      a2 += B::mont_lazy(v, w.z);
+      a3 += B::mont_lazy(v, w.w);
+    }
+    out[r] = make_uint4((uint32_t)(a0 % B::P), (uint32_t)(a1 % B::P), (uint32_t)(a2 % B::P),
+                        (uint32_t)(a3 % B::P));
+  }
+}
+
+static void ext4_mul_host(const uint32_t *a, const uint32_t *b, uint32_t *o) {
+  uint64_t c[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) c[i + j] = (c[i + j] + (uint64_t)a[i] * b[j]) % BabyBear::P;
+  for (int k = 0; k < 4; k++) o[k] = (uint32_t)((c[k] + 11 * (k + 4 < 7 ? c[k + 4] : 0)) % BabyBear::P);
+}
+
+int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
+                             const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s) {
+  ZKB_REQUIRE(((uintptr_t)d_out & 15) == 0, "output must be 16-byte aligned");
+  for (int k = 0; k < 4; k++) ZKB_REQUIRE(alpha[k] < BabyBear::P, "alpha is not canonical");
+  std::vector<uint32_t> pw((size_t)width * 4);
+  uint32_t cur[4] = {1, 0, 0, 0};
+  for (uint32_t j = 0; j < width; j++) {
+    for (int k = 0; k < 4; k++) pw[j * 4 + k] = BabyBear::tw_encode(cur[k]);
+    uint32_t nx[4];
+    ext4_mul_host(cur, alpha, nx);
+    for (int k = 0; k < 4; k++) cur[k] = nx[k];
+  }
+  ScratchBuf d_pw;
+  ZKB_TRY(d_pw.alloc(pw.size() * 4, s));
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(d_pw.p, pw.data(), pw.size() * 4, cudaMemcpyHostToDevice, s));
+  DeviceContext *ctx;
+  ZKB_TRY(current_context(&ctx));
+  ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<<<grid_for(rows, 256, (unsigned)ctx->sm_count * 8u), 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
+  // the host copy of the powers must outlive the asynchronous upload
+  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  return ZKB_OK;
+}
 
 }  // namespace zkb

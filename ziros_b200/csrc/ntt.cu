@@ -141,68 +141,150 @@ static int get_coset_table(int log_n, int log_b, typename F::T shift, const type
 }
 
 // -------------------------------------------------------------- pass kernel
+// One pass handles index bits [lo, lo+K) of every transform: for each fixed value of
+// the other bits (a "group") and each chunk of C columns, one CTA computes the
+// 2^K-point sub-DFT as a four-step inside the CTA:
+//   phase A: thread (i, c) loads the R1 = 2^LR1 elements x[j*R2 + i] of column c and
+//            runs an R1-point DIF in registers, multiplies by w_{2^K}^{i*f1} and
+//            writes them to shared memory, f1-major;
+//   phase B: thread (f1, c) reads its R2 = 2^LR2 values, runs an R2-point DIF in
+//            registers, applies the pass twist w_{2^hi}^{(row mod 2^lo)*f} (or the
+//            final 1/n scale) and stores at the bit-reversed tile position
+//            rev(f1)*R2 + t.
+// Register DIFs use compile-time indices and a 32-entry table of w_64 powers passed
+// as a kernel parameter, so a butterfly is one Montgomery multiply plus two adds.
 struct PassGeom {
   int L;                     // log2 of each transform
-  int lo, k;                 // index bits [lo, lo+k)
+  int lo;                    // lowest index bit of this pass
   uint32_t width;            // matrix columns
   uint32_t cols;             // columns per CTA (power of two dividing width)
   int log_cols;
   uint32_t chunks_per_row;   // width / cols
-  uint32_t groups;           // 2^(L-k) groups per transform
+  uint32_t groups;           // 2^(L-K) groups per transform
+  uint32_t sm_stride;        // shared-memory stride between f1 blocks (elements)
   uint64_t block_stride;     // elements between transforms
   int twist;
 };
 
 template <class F>
-__global__ void __launch_bounds__(256)
-    ntt_pass_kernel(const typename F::T *in, typename F::T *out, const PassGeom g,
-                    const typename F::T *__restrict__ tw, typename F::T post_scale) {
+struct SmallTw {
+  typename F::T w[32];  // w_64^e, e < 32, encoded for F::mul_tw
+};
+
+__host__ __device__ constexpr uint32_t rev_bits(uint32_t x, int bits) {
+  uint32_t r = 0;
+  for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+  return r;
+}
+
+// (a - b) * w for the DIF butterfly; BabyBear keeps a - b + p unreduced (< 2p), which
+// the lazy Montgomery product accepts.
+template <class F>
+__device__ __forceinline__ typename F::T dif_mul(typename F::T a, typename F::T b, typename F::T w);
+template <>
+__device__ __forceinline__ uint32_t dif_mul<BabyBear>(uint32_t a, uint32_t b, uint32_t w) {
+  return BabyBear::red(BabyBear::mont_lazy(a - b + BabyBear::P, w));
+}
+template <>
+__device__ __forceinline__ uint64_t dif_mul<Goldilocks>(uint64_t a, uint64_t b, uint64_t w) {
+  return Goldilocks::mul(Goldilocks::sub(a, b), w);
+}
+
+// In-register radix-2 DIF of 2^LR points: natural in, x[t] = X[rev(t)] out.
+template <class F, int LR>
+__device__ __forceinline__ void dif_reg(typename F::T (&x)[1 << LR], const typename F::T *w64) {
   using T = typename F::T;
+  constexpr int R = 1 << LR;
+#pragma unroll
+  for (int s = LR - 1; s >= 0; s--) {
+    const int h = 1 << s;
+#pragma unroll
+    for (int g = 0; g < R; g += 2 * h) {
+#pragma unroll
+      for (int j = 0; j < h; j++) {
+        T a = x[g + j], b = x[g + j + h];
+        x[g + j] = F::add(a, b);
+        x[g + j + h] = j == 0 ? F::sub(a, b) : dif_mul<F>(a, b, w64[j << (5 - s)]);
+      }
+    }
+  }
+}
+
+template <class F, int LR1, int LR2>
+__global__ void __launch_bounds__(512)
+    ntt_pass_kernel(const typename F::T *in, typename F::T *out, const PassGeom g,
+                    const typename F::T *__restrict__ tw, typename F::T post_scale,
+                    const __grid_constant__ SmallTw<F> st) {
+  using T = typename F::T;
+  constexpr int R1 = 1 << LR1, R2 = 1 << LR2, K = LR1 + LR2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *tile = reinterpret_cast<T *>(smem_raw);
-  const int k = g.k;
-  const int n_sub = 1 << k;
-  T *tws = tile + ((size_t)n_sub << g.log_cols);
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  // Twiddles shared by the C columns of the CTA, staged once:
+  //   tw_in[e]  = w_{2^K}^e            (phase-A twist, e = i * f1 < 2^K)
+  //   tw_out[f] = w_{2^hi}^{i_low * f} (pass twist), or the 1/n scale on the last pass
+  T *tw_in = sm + (size_t)g.sm_stride * R1;
+  T *tw_out = tw_in + (1 << K);
 
-  const uint64_t cta = blockIdx.x;
-  const uint32_t chunk = (uint32_t)(cta % g.chunks_per_row);
-  const uint64_t rest = cta / g.chunks_per_row;
-  const uint32_t grp = (uint32_t)(rest % g.groups);
-  const uint64_t blk = rest / g.groups;
-  const int hi = g.lo + k;
+  const uint32_t cta = blockIdx.x;
+  const uint32_t chunk = cta % g.chunks_per_row;
+  const uint32_t rest = cta / g.chunks_per_row;
+  const uint32_t grp = rest % g.groups;
+  const uint32_t blk = rest / g.groups;
+  const int hi = g.lo + K;
   const uint32_t i_low = grp & ((1u << g.lo) - 1u);
-  const uint64_t base_row = ((uint64_t)(grp >> g.lo) << hi) | i_low;
-  const size_t off = blk * g.block_stride + (size_t)chunk * g.cols;
-  const uint32_t C = g.cols, lc = g.log_cols;
+  const uint32_t base_row = ((grp >> g.lo) << hi) | i_low;
+  const uint32_t lc = g.log_cols;
+  const uint32_t c = threadIdx.x & (g.cols - 1);
+  const uint32_t i = threadIdx.x >> lc;  // < R2
+  const bool scale_out = g.twist || post_scale != 0;
 
-  for (int j = threadIdx.x; j < n_sub / 2; j += blockDim.x) tws[j] = tw[(size_t)j << (g.L - k)];
-  for (uint32_t e = threadIdx.x; e < ((uint32_t)n_sub << lc); e += blockDim.x) {
-    uint32_t t = e >> lc, c = e & (C - 1);
-    tile[e] = in[off + ((base_row + ((uint64_t)t << g.lo)) * g.width) + c];
+  for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) {
+    tw_in[e] = tw[e << (g.L - K)];
+    if (g.twist)
+      tw_out[e] = tw[(i_low * e) << (g.L - hi)];  // i_low * e < 2^hi <= 2^L
+    else if (post_scale)
+      tw_out[e] = post_scale;
+  }
+
+  const size_t col0 = (size_t)blk * g.block_stride + (size_t)chunk * g.cols + c;
+  const size_t rs = (size_t)g.width << g.lo;  // elements between consecutive tile rows
+  // ---- phase A
+  {
+    T x[R1];
+    const T *p = in + col0 + ((size_t)base_row * g.width) + (size_t)i * rs;
+    const size_t step = rs * R2;
+#pragma unroll
+    for (int j = 0; j < R1; j++) {
+      x[j] = *p;
+      p += step;
+    }
+    dif_reg<F, LR1>(x, st.w);
+    __syncthreads();  // tw_in staged
+#pragma unroll
+    for (int t = 0; t < R1; t++) {
+      const uint32_t f1 = rev_bits((uint32_t)t, LR1);
+      T v = x[t];
+      if (LR2 > 0 && f1 != 0) v = F::mul_tw(v, tw_in[i * f1]);
+      sm[f1 * g.sm_stride + (i << lc) + c] = v;
+    }
   }
   __syncthreads();
-  for (int s = k - 1; s >= 0; s--) {
-    const int half = 1 << s;
-    for (uint32_t e = threadIdx.x; e < ((uint32_t)(n_sub / 2) << lc); e += blockDim.x) {
-      uint32_t p = e >> lc, c = e & (C - 1);
-      uint32_t j = p & (half - 1);
-      uint32_t i0 = ((p >> s) << (s + 1)) | j;
-      T a = tile[(i0 << lc) + c], b = tile[((i0 + half) << lc) + c];
-      tile[(i0 << lc) + c] = F::add(a, b);
-      tile[((i0 + half) << lc) + c] = F::mul_tw(F::sub(a, b), tws[j << (k - 1 - s)]);
+  // ---- phase B
+#pragma unroll 1
+  for (int q = 0; q < R1 / R2; q++) {
+    const uint32_t f1 = i + q * R2;
+    T y[R2];
+#pragma unroll
+    for (int ii = 0; ii < R2; ii++) y[ii] = sm[f1 * g.sm_stride + (ii << lc) + c];
+    dif_reg<F, LR2>(y, st.w);
+    T *p = out + col0 + ((size_t)base_row * g.width) + (size_t)(rev_bits(f1, LR1) * R2) * rs;
+#pragma unroll
+    for (int t = 0; t < R2; t++) {
+      T v = y[t];
+      if (scale_out) v = F::mul_tw(v, tw_out[f1 + R1 * rev_bits((uint32_t)t, LR2)]);
+      *p = v;
+      p += rs;
     }
-    __syncthreads();
-  }
-  for (uint32_t e = threadIdx.x; e < ((uint32_t)n_sub << lc); e += blockDim.x) {
-    uint32_t t = e >> lc, c = e & (C - 1);
-    T v = tile[e];
-    if (g.twist) {
-      uint64_t f = __brev(t) >> (32 - k);
-      uint64_t ex = ((uint64_t)i_low * f) & ((1ull << hi) - 1);
-      v = F::mul_tw(v, tw[ex << (g.L - hi)]);
-    }
-    if (post_scale) v = F::mul_tw(v, post_scale);
-    out[off + ((base_row + ((uint64_t)t << g.lo)) * g.width) + c] = v;
   }
 }
 
@@ -224,42 +306,90 @@ static std::vector<int> plan_passes(int L, int kmax) {
 }
 
 template <class F>
+static SmallTw<F> small_twiddles(bool inverse) {
+  SmallTw<F> st;
+  typename F::T w = two_adic_generator<F>(6), acc = 1;
+  if (inverse) w = inv_host<F>(w);
+  for (int e = 0; e < 32; e++) {
+    st.w[e] = Dom<F>::encode(acc);
+    acc = F::mul_host(acc, w);
+  }
+  return st;
+}
+
+template <class F, int LR1, int LR2>
+static int launch_pass(const typename F::T *src, typename F::T *out, const PassGeom &g, uint64_t ctas,
+                       const typename F::T *tw, typename F::T scale, const SmallTw<F> &st,
+                       cudaStream_t s) {
+  using T = typename F::T;
+  const unsigned threads = g.cols << LR2;
+  const size_t smem = (((size_t)g.sm_stride << LR1) + (2u << (LR1 + LR2))) * sizeof(T);
+  ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<F, LR1, LR2>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  ZKB_LAUNCH("ntt_pass", s, ntt_pass_kernel<F, LR1, LR2><<<(unsigned)ctas, threads, smem, s>>>(src, out, g, tw, scale, st));
+  return ZKB_OK;
+}
+
+template <class F>
 static int run_passes(const typename F::T *in, typename F::T *out, int L, uint32_t width,
-                      uint64_t n_blocks, const typename F::T *tw, typename F::T last_scale,
-                      cudaStream_t s) {
+                      uint64_t n_blocks, const typename F::T *tw, bool inverse,
+                      typename F::T last_scale, cudaStream_t s) {
   using T = typename F::T;
   const uint32_t C = pick_cols<F>(width);
   int lc = 0;
   while ((1u << lc) < C) lc++;
-  // tile of at most 64 KiB
-  int kmax = 0;
-  while (((size_t)sizeof(T) << (kmax + 1 + lc)) <= 65536 && kmax + 1 <= 12) kmax++;
+  // BabyBear: up to 64 + 32 registers of data per thread phase; Goldilocks: 32 + 32.
+  const int kmax = sizeof(T) == 4 ? 11 : 10;
   std::vector<int> ks = plan_passes(L, kmax);
-  ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<F>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  // the register DIFs use w_64 of the same direction as the table `tw`
+  const SmallTw<F> st = small_twiddles<F>(inverse);
   int hi = L;
   const T *src = in;
   for (size_t pi = 0; pi < ks.size(); pi++) {
+    const int K = ks[pi];
     PassGeom g;
     g.L = L;
-    g.k = ks[pi];
-    g.lo = hi - g.k;
+    g.lo = hi - K;
     g.width = width;
     g.cols = C;
     g.log_cols = lc;
     g.chunks_per_row = width / C;
-    g.groups = 1u << (L - g.k);
+    g.groups = 1u << (L - K);
+    // stride between f1 blocks = R2*C padded to = C (mod 32) elements: the warps of
+    // phase B read two or more f1 blocks at once without bank conflicts
+    uint32_t base = C << (K / 2);
+    g.sm_stride = base + ((C - (base % 32u)) % 32u);
     g.block_stride = ((uint64_t)width) << L;
     g.twist = g.lo > 0;
-    uint64_t ctas = (uint64_t)g.chunks_per_row * g.groups * n_blocks;
-    if (ctas >= (1ull << 31)) {
+    const uint64_t ctas = (uint64_t)g.chunks_per_row * g.groups * n_blocks;
+    if (ctas >= (1ull << 31) || ((uint64_t)width << L) * n_blocks >= (1ull << 40)) {
       set_error("NTT launch too large");
       return ZKB_ERR_UNSUPPORTED;
     }
-    size_t smem = (((size_t)1 << g.k) << lc) * sizeof(T) + ((size_t)1 << (g.k - 1)) * sizeof(T);
-    T scale = (pi + 1 == ks.size()) ? last_scale : (T)0;
-    ZKB_LAUNCH("ntt_pass", s, ntt_pass_kernel<F><<<(unsigned)ctas, 256, smem, s>>>(src, out, g, tw, scale));
-    ZKB_CHECK_LAUNCH();
+    const T scale = (pi + 1 == ks.size()) ? last_scale : (T)0;
+    int rc;
+    switch (K) {
+      case 1: rc = launch_pass<F, 1, 0>(src, out, g, ctas, tw, scale, st, s); break;
+      case 2: rc = launch_pass<F, 1, 1>(src, out, g, ctas, tw, scale, st, s); break;
+      case 3: rc = launch_pass<F, 2, 1>(src, out, g, ctas, tw, scale, st, s); break;
+      case 4: rc = launch_pass<F, 2, 2>(src, out, g, ctas, tw, scale, st, s); break;
+      case 5: rc = launch_pass<F, 3, 2>(src, out, g, ctas, tw, scale, st, s); break;
+      case 6: rc = launch_pass<F, 3, 3>(src, out, g, ctas, tw, scale, st, s); break;
+      case 7: rc = launch_pass<F, 4, 3>(src, out, g, ctas, tw, scale, st, s); break;
+      case 8: rc = launch_pass<F, 4, 4>(src, out, g, ctas, tw, scale, st, s); break;
+      case 9: rc = launch_pass<F, 5, 4>(src, out, g, ctas, tw, scale, st, s); break;
+      case 10: rc = launch_pass<F, 5, 5>(src, out, g, ctas, tw, scale, st, s); break;
+      case 11:
+        if constexpr (sizeof(T) == 4) {
+          rc = launch_pass<F, 6, 5>(src, out, g, ctas, tw, scale, st, s);
+          break;
+        }
+        [[fallthrough]];
+      default:
+        set_error("internal: NTT pass of %d bits", K);
+        return ZKB_ERR_INTERNAL;
+    }
+    ZKB_TRY(rc);
     src = out;
     hi = g.lo;
   }
@@ -308,7 +438,7 @@ int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaS
   ZKB_TRY(tmp.alloc(n * width * sizeof(T), s));
   T scale = 0;
   if (inverse) scale = Dom<F>::encode(inv_host<F>((T)(n % (uint64_t)F::P)));
-  ZKB_TRY(run_passes<F>(d, tmp.as<T>(), log_h, width, 1, tw, scale, s));
+  ZKB_TRY(run_passes<F>(d, tmp.as<T>(), log_h, width, 1, tw, inverse, scale, s));
   ZKB_LAUNCH("bitrev_rows", s, bitrev_rows_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(tmp.as<T>(), d, log_h, width,
                                                                    n * width));
   ZKB_CHECK_LAUNCH();
@@ -330,7 +460,7 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
   if (log_h > 0) {
     const T *itw;
     ZKB_TRY(get_twiddles<F>(log_h, true, &itw, s));
-    ZKB_TRY(run_passes<F>(d_trace, coef.as<T>(), log_h, width, 1, itw, (T)0, s));
+    ZKB_TRY(run_passes<F>(d_trace, coef.as<T>(), log_h, width, 1, itw, true, (T)0, s));
   } else {
     ZKB_CHECK_CUDA(cudaMemcpyAsync(coef.p, d_trace, width * sizeof(T), cudaMemcpyDeviceToDevice, s));
   }
@@ -342,7 +472,7 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
   if (log_h > 0) {
     const T *tw;
     ZKB_TRY(get_twiddles<F>(log_h, false, &tw, s));
-    ZKB_TRY(run_passes<F>(d_out, d_out, log_h, width, 1ull << log_b, tw, (T)0, s));
+    ZKB_TRY(run_passes<F>(d_out, d_out, log_h, width, 1ull << log_b, tw, false, (T)0, s));
   }
   if (!bitrev) {
     const int LN = log_h + log_b;
@@ -370,7 +500,7 @@ int ntt_dft_into(typename F::T *d, int log_h, uint32_t width, bool inverse, type
   ZKB_TRY(launch_powers<F>(tw_buf, n, w, 1, s));
   T scale = 0;
   if (inverse) scale = Dom<F>::encode(inv_host<F>((T)(n % (uint64_t)F::P)));
-  ZKB_TRY(run_passes<F>(d, tmp, log_h, width, 1, tw_buf, scale, s));
+  ZKB_TRY(run_passes<F>(d, tmp, log_h, width, 1, tw_buf, inverse, scale, s));
   ZKB_LAUNCH("bitrev_rows", s, bitrev_rows_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(tmp, d, log_h, width, n * width));
   return ZKB_OK;
 }

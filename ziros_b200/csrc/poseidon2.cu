@@ -22,6 +22,13 @@ bool build_p2_params(const uint64_t *rc, size_t n_rc, int rounds_f, int rounds_p
   p->rounds_p = rounds_p;
   p->out = out;
   p->rate = 8;
+  p->diag_kind = 0;
+  if (sizeof(typename F::T) == 4 && W == 16) {
+    std::vector<uint64_t> v = p2_diagonal(FIELD_BABYBEAR, 16);
+    bool same = true;
+    for (int i = 0; i < W; i++) same = same && diag[i] == v[i];
+    p->diag_kind = same ? 1 : 0;
+  }
   return true;
 }
 
