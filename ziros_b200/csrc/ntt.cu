@@ -21,6 +21,8 @@
 //
 // i.e. b independent size-n NR transforms of the coefficients twisted per coset.
 #include <algorithm>
+#include <type_traits>
+#include <utility>
 
 #include "common.cuh"
 #include "engine.cuh"
@@ -157,11 +159,8 @@ struct PassGeom {
   int L;                     // log2 of each transform
   int lo;                    // lowest index bit of this pass
   uint32_t width;            // matrix columns
-  uint32_t cols;             // columns per CTA (power of two dividing width)
-  int log_cols;
-  uint32_t chunks_per_row;   // width / cols
+  uint32_t chunks_per_row;   // width / C
   uint32_t groups;           // 2^(L-K) groups per transform
-  uint32_t sm_stride;        // shared-memory stride between f1 blocks (elements)
   uint64_t block_stride;     // elements between transforms
   int twist;
 };
@@ -171,9 +170,9 @@ struct SmallTw {
   typename F::T w[32];  // w_64^e, e < 32, encoded for F::mul_tw
 };
 
-__host__ __device__ constexpr uint32_t rev_bits(uint32_t x, int bits) {
-  uint32_t r = 0;
-  for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+__host__ __device__ constexpr int rev_bits(int x, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; i++) r |= ((x >> i) & 1) << (bits - 1 - i);
   return r;
 }
 
@@ -190,39 +189,60 @@ __device__ __forceinline__ uint64_t dif_mul<Goldilocks>(uint64_t a, uint64_t b, 
   return Goldilocks::mul(Goldilocks::sub(a, b), w);
 }
 
-// In-register radix-2 DIF of 2^LR points: natural in, x[t] = X[rev(t)] out.
-template <class F, int LR>
-__device__ __forceinline__ void dif_reg(typename F::T (&x)[1 << LR], const typename F::T *w64) {
-  using T = typename F::T;
-  constexpr int R = 1 << LR;
-#pragma unroll
-  for (int s = LR - 1; s >= 0; s--) {
-    const int h = 1 << s;
-#pragma unroll
-    for (int g = 0; g < R; g += 2 * h) {
-#pragma unroll
-      for (int j = 0; j < h; j++) {
-        T a = x[g + j], b = x[g + j + h];
-        x[g + j] = F::add(a, b);
-        x[g + j + h] = j == 0 ? F::sub(a, b) : dif_mul<F>(a, b, w64[j << (5 - s)]);
-      }
-    }
-  }
+// Compile-time loop: fn(std::integral_constant<int, I>) for I = 0..N-1, so every index
+// derived from I (bit reversals, twiddle slots) is a constant expression.
+template <class Fn, int... I>
+__device__ __forceinline__ void sfor_impl(Fn &fn, std::integer_sequence<int, I...>) {
+  (fn(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class Fn>
+__device__ __forceinline__ void sfor(Fn &&fn) {
+  if constexpr (N > 0) sfor_impl(fn, std::make_integer_sequence<int, N>{});
 }
 
-template <class F, int LR1, int LR2>
-__global__ void __launch_bounds__(512)
+// In-register radix-2 DIF of 2^LR points: natural in, x[t] = X[rev(t)] out.
+template <class F, int LR>
+__device__ __forceinline__ void dif_reg(typename F::T (&x)[1 << LR], const SmallTw<F> &st) {
+  using T = typename F::T;
+  sfor<LR>([&](auto sc) {
+    constexpr int s = LR - 1 - decltype(sc)::value;
+    constexpr int h = 1 << s;
+    sfor<(1 << LR) / 2>([&](auto bc) {
+      constexpr int b = decltype(bc)::value;
+      constexpr int j = b % h, g = (b / h) * 2 * h;
+      const T a = x[g + j], c = x[g + j + h];
+      x[g + j] = F::add(a, c);
+      if constexpr (j == 0)
+        x[g + j + h] = F::sub(a, c);
+      else
+        x[g + j + h] = dif_mul<F>(a, c, st.w[j << (5 - s)]);
+    });
+  });
+}
+
+// Shared-memory geometry of a pass with C columns per CTA: f1 blocks of R2*C values,
+// padded so the stride is = C (mod 32) words and phase-B warps reading several f1
+// blocks hit distinct banks.
+template <int LR2, int C>
+struct PassSmem {
+  static constexpr int BASE = C << LR2;
+  static constexpr int STRIDE = BASE + ((C - (BASE % 32)) % 32 + 32) % 32;
+};
+
+template <class F, int LR1, int LR2, int C>
+__global__ void __launch_bounds__(C << LR2)
     ntt_pass_kernel(const typename F::T *in, typename F::T *out, const PassGeom g,
                     const typename F::T *__restrict__ tw, typename F::T post_scale,
                     const __grid_constant__ SmallTw<F> st) {
   using T = typename F::T;
   constexpr int R1 = 1 << LR1, R2 = 1 << LR2, K = LR1 + LR2;
+  constexpr int S = PassSmem<LR2, C>::STRIDE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
   // Twiddles shared by the C columns of the CTA, staged once:
-  //   tw_in[e]  = w_{2^K}^e            (phase-A twist, e = i * f1 < 2^K)
-  //   tw_out[f] = w_{2^hi}^{i_low * f} (pass twist), or the 1/n scale on the last pass
-  T *tw_in = sm + (size_t)g.sm_stride * R1;
+  //   tw_in[i*R1 + t]  = w_{2^K}^{i * rev(t)}   (phase-A twist of output t of thread i)
+  //   tw_out[f]        = w_{2^hi}^{i_low * f}  (pass twist), or the 1/n scale on the last pass
+  T *tw_in = sm + S * R1;
   T *tw_out = tw_in + (1 << K);
 
   const uint32_t cta = blockIdx.x;
@@ -233,21 +253,22 @@ __global__ void __launch_bounds__(512)
   const int hi = g.lo + K;
   const uint32_t i_low = grp & ((1u << g.lo) - 1u);
   const uint32_t base_row = ((grp >> g.lo) << hi) | i_low;
-  const uint32_t lc = g.log_cols;
-  const uint32_t c = threadIdx.x & (g.cols - 1);
-  const uint32_t i = threadIdx.x >> lc;  // < R2
+  const uint32_t c = threadIdx.x % C;
+  const uint32_t i = threadIdx.x / C;  // < R2
   const bool scale_out = g.twist || post_scale != 0;
 
   for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) {
-    tw_in[e] = tw[e << (g.L - K)];
+    const uint32_t ii = e / R1, tt = e % R1;
+    tw_in[e] = tw[(ii * (__brev(tt) >> (32 - LR1))) << (g.L - K)];
     if (g.twist)
       tw_out[e] = tw[(i_low * e) << (g.L - hi)];  // i_low * e < 2^hi <= 2^L
     else if (post_scale)
       tw_out[e] = post_scale;
   }
 
-  const size_t col0 = (size_t)blk * g.block_stride + (size_t)chunk * g.cols + c;
+  const size_t col0 = (size_t)blk * g.block_stride + (size_t)chunk * C + c;
   const size_t rs = (size_t)g.width << g.lo;  // elements between consecutive tile rows
+  T *sm_a = sm + i * C + c;                    // phase A: + f1 * S
   // ---- phase A
   {
     T x[R1];
@@ -258,42 +279,44 @@ __global__ void __launch_bounds__(512)
       x[j] = *p;
       p += step;
     }
-    dif_reg<F, LR1>(x, st.w);
+    dif_reg<F, LR1>(x, st);
     __syncthreads();  // tw_in staged
-#pragma unroll
-    for (int t = 0; t < R1; t++) {
-      const uint32_t f1 = rev_bits((uint32_t)t, LR1);
+    const T *twi = tw_in + i * R1;
+    sfor<R1>([&](auto tc) {
+      constexpr int t = decltype(tc)::value;
       T v = x[t];
-      if (LR2 > 0 && f1 != 0) v = F::mul_tw(v, tw_in[i * f1]);
-      sm[f1 * g.sm_stride + (i << lc) + c] = v;
-    }
+      if constexpr (LR2 > 0 && t != 0) v = F::mul_tw(v, twi[t]);
+      sm_a[rev_bits(t, LR1) * S] = v;
+    });
   }
   __syncthreads();
   // ---- phase B
 #pragma unroll 1
   for (int q = 0; q < R1 / R2; q++) {
     const uint32_t f1 = i + q * R2;
+    const T *sm_b = sm + f1 * S + c;
     T y[R2];
 #pragma unroll
-    for (int ii = 0; ii < R2; ii++) y[ii] = sm[f1 * g.sm_stride + (ii << lc) + c];
-    dif_reg<F, LR2>(y, st.w);
-    T *p = out + col0 + ((size_t)base_row * g.width) + (size_t)(rev_bits(f1, LR1) * R2) * rs;
-#pragma unroll
-    for (int t = 0; t < R2; t++) {
+    for (int ii = 0; ii < R2; ii++) y[ii] = sm_b[ii * C];
+    dif_reg<F, LR2>(y, st);
+    T *p = out + col0 + ((size_t)base_row * g.width) + (size_t)((__brev(f1) >> (32 - LR1)) * R2) * rs;
+    const T *two = tw_out + f1;
+    sfor<R2>([&](auto tc) {
+      constexpr int t = decltype(tc)::value;
       T v = y[t];
-      if (scale_out) v = F::mul_tw(v, tw_out[f1 + R1 * rev_bits((uint32_t)t, LR2)]);
+      if (scale_out) v = F::mul_tw(v, two[R1 * rev_bits(t, LR2)]);
       *p = v;
       p += rs;
-    }
+    });
   }
 }
 
 template <class F>
 static uint32_t pick_cols(uint32_t width) {
-  uint32_t cmax = sizeof(typename F::T) == 4 ? 16 : 8;
-  uint32_t c = 1;
-  while (c * 2 <= cmax && width % (c * 2) == 0) c *= 2;
-  return c;
+  if (sizeof(typename F::T) == 4 && width % 16 == 0) return 16;
+  if (width % 8 == 0) return 8;
+  if (width % 4 == 0) return 4;
+  return 1;
 }
 
 // Split L bits into passes of at most kmax bits, as even as possible, top first.
@@ -317,33 +340,53 @@ static SmallTw<F> small_twiddles(bool inverse) {
   return st;
 }
 
-template <class F, int LR1, int LR2>
-static int launch_pass(const typename F::T *src, typename F::T *out, const PassGeom &g, uint64_t ctas,
-                       const typename F::T *tw, typename F::T scale, const SmallTw<F> &st,
-                       cudaStream_t s) {
+template <class F, int LR1, int LR2, int C>
+static int launch_pass_c(const typename F::T *src, typename F::T *out, const PassGeom &g, uint64_t ctas,
+                         const typename F::T *tw, typename F::T scale, const SmallTw<F> &st,
+                         cudaStream_t s) {
   using T = typename F::T;
-  const unsigned threads = g.cols << LR2;
-  const size_t smem = (((size_t)g.sm_stride << LR1) + (2u << (LR1 + LR2))) * sizeof(T);
-  ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<F, LR1, LR2>,
+  constexpr unsigned threads = C << LR2;
+  const size_t smem = ((size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) + (2u << (LR1 + LR2))) * sizeof(T);
+  ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<F, LR1, LR2, C>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  ZKB_LAUNCH("ntt_pass", s, ntt_pass_kernel<F, LR1, LR2><<<(unsigned)ctas, threads, smem, s>>>(src, out, g, tw, scale, st));
+  ZKB_LAUNCH("ntt_pass", s, ntt_pass_kernel<F, LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(src, out, g, tw, scale, st));
   return ZKB_OK;
 }
 
+template <class F, int LR1, int LR2>
+static int launch_pass(const typename F::T *src, typename F::T *out, const PassGeom &g, uint64_t ctas,
+                       const typename F::T *tw, typename F::T scale, const SmallTw<F> &st,
+                       uint32_t C, cudaStream_t s) {
+  switch (C) {
+    case 16:
+      if constexpr (sizeof(typename F::T) == 4) return launch_pass_c<F, LR1, LR2, 16>(src, out, g, ctas, tw, scale, st, s);
+      break;
+    case 8: return launch_pass_c<F, LR1, LR2, 8>(src, out, g, ctas, tw, scale, st, s);
+    case 4: return launch_pass_c<F, LR1, LR2, 4>(src, out, g, ctas, tw, scale, st, s);
+    case 1: return launch_pass_c<F, LR1, LR2, 1>(src, out, g, ctas, tw, scale, st, s);
+    default: break;
+  }
+  set_error("internal: NTT column chunk %u", C);
+  return ZKB_ERR_INTERNAL;
+}
+
+// Largest pass: BabyBear up to 64 + 32 values per thread phase, Goldilocks 32 + 32.
 template <class F>
-static int run_passes(const typename F::T *in, typename F::T *out, int L, uint32_t width,
-                      uint64_t n_blocks, const typename F::T *tw, bool inverse,
-                      typename F::T last_scale, cudaStream_t s) {
+static constexpr int pass_kmax() {
+  return sizeof(typename F::T) == 4 ? 11 : 10;
+}
+
+// Runs the passes `ks` (bit counts, top first) starting at index bit hi_start.
+template <class F>
+static int run_plan(const typename F::T *in, typename F::T *out, int L, uint32_t width,
+                    uint64_t n_blocks, const typename F::T *tw, bool inverse,
+                    typename F::T last_scale, const std::vector<int> &ks, int hi_start,
+                    cudaStream_t s) {
   using T = typename F::T;
   const uint32_t C = pick_cols<F>(width);
-  int lc = 0;
-  while ((1u << lc) < C) lc++;
-  // BabyBear: up to 64 + 32 registers of data per thread phase; Goldilocks: 32 + 32.
-  const int kmax = sizeof(T) == 4 ? 11 : 10;
-  std::vector<int> ks = plan_passes(L, kmax);
   // the register DIFs use w_64 of the same direction as the table `tw`
   const SmallTw<F> st = small_twiddles<F>(inverse);
-  int hi = L;
+  int hi = hi_start;
   const T *src = in;
   for (size_t pi = 0; pi < ks.size(); pi++) {
     const int K = ks[pi];
@@ -351,14 +394,8 @@ static int run_passes(const typename F::T *in, typename F::T *out, int L, uint32
     g.L = L;
     g.lo = hi - K;
     g.width = width;
-    g.cols = C;
-    g.log_cols = lc;
     g.chunks_per_row = width / C;
     g.groups = 1u << (L - K);
-    // stride between f1 blocks = R2*C padded to = C (mod 32) elements: the warps of
-    // phase B read two or more f1 blocks at once without bank conflicts
-    uint32_t base = C << (K / 2);
-    g.sm_stride = base + ((C - (base % 32u)) % 32u);
     g.block_stride = ((uint64_t)width) << L;
     g.twist = g.lo > 0;
     const uint64_t ctas = (uint64_t)g.chunks_per_row * g.groups * n_blocks;
@@ -369,19 +406,19 @@ static int run_passes(const typename F::T *in, typename F::T *out, int L, uint32
     const T scale = (pi + 1 == ks.size()) ? last_scale : (T)0;
     int rc;
     switch (K) {
-      case 1: rc = launch_pass<F, 1, 0>(src, out, g, ctas, tw, scale, st, s); break;
-      case 2: rc = launch_pass<F, 1, 1>(src, out, g, ctas, tw, scale, st, s); break;
-      case 3: rc = launch_pass<F, 2, 1>(src, out, g, ctas, tw, scale, st, s); break;
-      case 4: rc = launch_pass<F, 2, 2>(src, out, g, ctas, tw, scale, st, s); break;
-      case 5: rc = launch_pass<F, 3, 2>(src, out, g, ctas, tw, scale, st, s); break;
-      case 6: rc = launch_pass<F, 3, 3>(src, out, g, ctas, tw, scale, st, s); break;
-      case 7: rc = launch_pass<F, 4, 3>(src, out, g, ctas, tw, scale, st, s); break;
-      case 8: rc = launch_pass<F, 4, 4>(src, out, g, ctas, tw, scale, st, s); break;
-      case 9: rc = launch_pass<F, 5, 4>(src, out, g, ctas, tw, scale, st, s); break;
-      case 10: rc = launch_pass<F, 5, 5>(src, out, g, ctas, tw, scale, st, s); break;
+      case 1: rc = launch_pass<F, 1, 0>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 2: rc = launch_pass<F, 1, 1>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 3: rc = launch_pass<F, 2, 1>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 4: rc = launch_pass<F, 2, 2>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 5: rc = launch_pass<F, 3, 2>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 6: rc = launch_pass<F, 3, 3>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 7: rc = launch_pass<F, 4, 3>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 8: rc = launch_pass<F, 4, 4>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 9: rc = launch_pass<F, 5, 4>(src, out, g, ctas, tw, scale, st, C, s); break;
+      case 10: rc = launch_pass<F, 5, 5>(src, out, g, ctas, tw, scale, st, C, s); break;
       case 11:
         if constexpr (sizeof(T) == 4) {
-          rc = launch_pass<F, 6, 5>(src, out, g, ctas, tw, scale, st, s);
+          rc = launch_pass<F, 6, 5>(src, out, g, ctas, tw, scale, st, C, s);
           break;
         }
         [[fallthrough]];
@@ -394,6 +431,174 @@ static int run_passes(const typename F::T *in, typename F::T *out, int L, uint32
     hi = g.lo;
   }
   return ZKB_OK;
+}
+
+template <class F>
+static int run_passes(const typename F::T *in, typename F::T *out, int L, uint32_t width,
+                      uint64_t n_blocks, const typename F::T *tw, bool inverse,
+                      typename F::T last_scale, cudaStream_t s) {
+  return run_plan<F>(in, out, L, width, n_blocks, tw, inverse, last_scale,
+                     plan_passes(L, pass_kmax<F>()), L, s);
+}
+
+// --------------------------------------------------------- fused LDE middle
+// One kernel for the last pass of the inverse transform (bits [0, K), contiguous row
+// blocks B), the coset twist c_m * (s w_bn^j)^m / n of every coset j, and the first pass
+// of each coset's forward transform (bits [L-K, L)).  After the inverse pass the
+// coefficients of block B are c[m] with m = m_hi * 2^(L-K) + m_lo, m_lo = rev(B) fixed,
+// and — as the forward pass splits m_hi = j' * R2 + i exactly like the inverse pass's
+// phase B holds them — each thread already has the R1 coefficients its forward phase A
+// needs, so the coefficient matrix never goes back to HBM and no expand pass runs.
+struct FusedGeom {
+  int L;
+  uint32_t width;
+  uint32_t chunks_per_row;
+  uint32_t blocks;   // 2^(L-K)
+  int log_b;
+  uint64_t n;        // 2^L
+};
+
+template <class F, int LR1, int LR2, int C>
+__global__ void __launch_bounds__(C << LR2)
+    lde_fused_kernel(const typename F::T *in, typename F::T *out, const FusedGeom g,
+                     const typename F::T *__restrict__ itw, const typename F::T *__restrict__ ftw,
+                     const typename F::T *__restrict__ ctab, const __grid_constant__ SmallTw<F> ist,
+                     const __grid_constant__ SmallTw<F> fst) {
+  using T = typename F::T;
+  constexpr int R1 = 1 << LR1, R2 = 1 << LR2, K = LR1 + LR2, Q = R1 / R2;
+  constexpr int S = PassSmem<LR2, C>::STRIDE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  T *itw_in = sm + S * R1;        // [i][t] inverse inner twist
+  T *ftw_in = itw_in + (1 << K);  // [i][t] forward inner twist
+  T *ftw_out = ftw_in + (1 << K); // w_{2^L}^{m_lo * f}
+  T *cf = ftw_out + (1 << K);     // coset factors of the current coset
+
+  const uint32_t cta = blockIdx.x;
+  const uint32_t chunk = cta % g.chunks_per_row;
+  const uint32_t B = cta / g.chunks_per_row;
+  const int lm = g.L - K;  // bits of m_lo
+  const uint32_t m_lo = lm ? (__brev(B) >> (32 - lm)) : 0u;
+  const uint32_t c = threadIdx.x % C;
+  const uint32_t i = threadIdx.x / C;
+
+  for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) {
+    const uint32_t ii = e / R1, tt = e % R1;
+    const uint32_t ex = (ii * (__brev(tt) >> (32 - LR1))) << lm;
+    itw_in[e] = itw[ex];
+    ftw_in[e] = ftw[ex];
+    ftw_out[e] = ftw[m_lo * e];  // < 2^L
+  }
+
+  const size_t colc = (size_t)chunk * C + c;
+  T *sm_a = sm + i * C + c;
+  // ---- inverse pass over the contiguous block B (no twist: lowest bits)
+  T coef[R1];
+  {
+    T x[R1];
+    const T *p = in + colc + ((size_t)B * (1u << K) + i) * g.width;
+    const size_t step = (size_t)R2 * g.width;
+#pragma unroll
+    for (int j = 0; j < R1; j++) {
+      x[j] = *p;
+      p += step;
+    }
+    dif_reg<F, LR1>(x, ist);
+    __syncthreads();
+    const T *twi = itw_in + i * R1;
+    sfor<R1>([&](auto tc) {
+      constexpr int t = decltype(tc)::value;
+      T v = x[t];
+      if constexpr (LR2 > 0 && t != 0) v = F::mul_tw(v, twi[t]);
+      sm_a[rev_bits(t, LR1) * S] = v;
+    });
+  }
+  __syncthreads();
+  sfor<Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const T *sm_b = sm + (i + q * R2) * S + c;
+    T y[R2];
+#pragma unroll
+    for (int ii = 0; ii < R2; ii++) y[ii] = sm_b[ii * C];
+    dif_reg<F, LR2>(y, ist);
+    sfor<R2>([&](auto tc) {
+      constexpr int t = decltype(tc)::value;
+      coef[rev_bits(t, LR2) * Q + q] = y[t];
+    });
+  });
+  // ---- per coset: twist, forward pass over bits [L-K, L)
+  const size_t rs = (size_t)g.width << lm;
+  for (int jc = 0; jc < (1 << g.log_b); jc++) {
+    __syncthreads();  // previous users of the tile and of cf are done
+    const T *ct = ctab + (uint64_t)jc * g.n + m_lo;
+    for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) cf[e] = ct[(uint64_t)e << lm];
+    __syncthreads();
+    {
+      T x[R1];
+#pragma unroll
+      for (int j = 0; j < R1; j++) x[j] = F::mul_tw(coef[j], cf[j * R2 + i]);
+      dif_reg<F, LR1>(x, fst);
+      const T *twi = ftw_in + i * R1;
+      sfor<R1>([&](auto tc) {
+        constexpr int t = decltype(tc)::value;
+        T v = x[t];
+        if constexpr (LR2 > 0 && t != 0) v = F::mul_tw(v, twi[t]);
+        sm_a[rev_bits(t, LR1) * S] = v;
+      });
+    }
+    __syncthreads();
+    const uint32_t r = g.log_b ? (__brev((uint32_t)jc) >> (32 - g.log_b)) : 0u;
+    T *blk = out + (uint64_t)r * g.n * g.width + colc + (size_t)m_lo * g.width;
+#pragma unroll 1
+    for (int q = 0; q < Q; q++) {
+      const uint32_t f1 = i + q * R2;
+      const T *sm_b = sm + f1 * S + c;
+      T y[R2];
+#pragma unroll
+      for (int ii = 0; ii < R2; ii++) y[ii] = sm_b[ii * C];
+      dif_reg<F, LR2>(y, fst);
+      T *p = blk + (size_t)((__brev(f1) >> (32 - LR1)) * R2) * rs;
+      const T *two = ftw_out + f1;
+      sfor<R2>([&](auto tc) {
+        constexpr int t = decltype(tc)::value;
+        T v = y[t];
+        if (lm > 0) v = F::mul_tw(v, two[R1 * rev_bits(t, LR2)]);
+        *p = v;
+        p += rs;
+      });
+    }
+  }
+}
+
+template <class F, int LR1, int LR2, int C>
+static int launch_fused_c(const typename F::T *in, typename F::T *out, const FusedGeom &g,
+                          const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
+                          cudaStream_t s) {
+  using T = typename F::T;
+  constexpr unsigned threads = C << LR2;
+  const size_t smem = ((size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) + (4u << (LR1 + LR2))) * sizeof(T);
+  ZKB_CHECK_CUDA(cudaFuncSetAttribute(lde_fused_kernel<F, LR1, LR2, C>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  const uint64_t ctas = (uint64_t)g.chunks_per_row * g.blocks;
+  const SmallTw<F> ist = small_twiddles<F>(true), fst = small_twiddles<F>(false);
+  ZKB_LAUNCH("lde_fused", s, lde_fused_kernel<F, LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(in, out, g, itw, ftw, ctab, ist, fst));
+  return ZKB_OK;
+}
+
+// Column chunk of the fused kernel: it holds 2 x R1 values per thread, so BabyBear uses
+// 8 columns (256 threads, up to 255 registers) where the plain passes use 16.
+template <class F, int LR1, int LR2>
+static int launch_fused(const typename F::T *in, typename F::T *out, const FusedGeom &g,
+                        const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
+                        uint32_t C, cudaStream_t s) {
+  switch (C) {
+    case 8: return launch_fused_c<F, LR1, LR2, 8>(in, out, g, itw, ftw, ctab, s);
+    case 4: return launch_fused_c<F, LR1, LR2, 4>(in, out, g, itw, ftw, ctab, s);
+    case 1: return launch_fused_c<F, LR1, LR2, 1>(in, out, g, itw, ftw, ctab, s);
+    default: break;
+  }
+  set_error("internal: fused LDE column chunk %u", C);
+  return ZKB_ERR_INTERNAL;
 }
 
 // ------------------------------------------------------- auxiliary kernels
@@ -446,6 +651,35 @@ int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaS
 }
 
 template <class F>
+static int launch_fused_k(int K, const typename F::T *in, typename F::T *out, const FusedGeom &g,
+                          const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
+                          uint32_t C, cudaStream_t s) {
+  switch (K) {
+    case 1: return launch_fused<F, 1, 0>(in, out, g, itw, ftw, ctab, C, s);
+    case 2: return launch_fused<F, 1, 1>(in, out, g, itw, ftw, ctab, C, s);
+    case 3: return launch_fused<F, 2, 1>(in, out, g, itw, ftw, ctab, C, s);
+    case 4: return launch_fused<F, 2, 2>(in, out, g, itw, ftw, ctab, C, s);
+    case 5: return launch_fused<F, 3, 2>(in, out, g, itw, ftw, ctab, C, s);
+    case 6: return launch_fused<F, 3, 3>(in, out, g, itw, ftw, ctab, C, s);
+    case 7: return launch_fused<F, 4, 3>(in, out, g, itw, ftw, ctab, C, s);
+    case 8: return launch_fused<F, 4, 4>(in, out, g, itw, ftw, ctab, C, s);
+    case 9: return launch_fused<F, 5, 4>(in, out, g, itw, ftw, ctab, C, s);
+    case 10: return launch_fused<F, 5, 5>(in, out, g, itw, ftw, ctab, C, s);
+    case 11:
+      if constexpr (sizeof(typename F::T) == 4) return launch_fused<F, 6, 5>(in, out, g, itw, ftw, ctab, C, s);
+      [[fallthrough]];
+    default:
+      set_error("internal: fused LDE pass of %d bits", K);
+      return ZKB_ERR_INTERNAL;
+  }
+}
+
+// Coset LDE, rows bit-reversed (the PCS order):
+//   inverse passes over all but the lowest K bits (trace -> coefficient scratch),
+//   lde_fused_kernel (last inverse pass + coset twists + first forward pass),
+//   the remaining forward passes in place on the 2^log_b coset blocks,
+// with the forward plan the mirror of the inverse one so both meet at K bits.
+template <class F>
 int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log_b,
                 typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s) {
   using T = typename F::T;
@@ -455,24 +689,42 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
     return ZKB_ERR_INVALID;
   }
   const uint64_t n = 1ull << log_h;
-  ScratchBuf coef;
-  ZKB_TRY(coef.alloc(n * width * sizeof(T), s));
-  if (log_h > 0) {
-    const T *itw;
-    ZKB_TRY(get_twiddles<F>(log_h, true, &itw, s));
-    ZKB_TRY(run_passes<F>(d_trace, coef.as<T>(), log_h, width, 1, itw, true, (T)0, s));
-  } else {
-    ZKB_CHECK_CUDA(cudaMemcpyAsync(coef.p, d_trace, width * sizeof(T), cudaMemcpyDeviceToDevice, s));
-  }
   const T *ctab;
   ZKB_TRY(get_coset_table<F>(log_h, log_b, shift, &ctab, s));
-  ZKB_LAUNCH("lde_expand", s, lde_expand_kernel<F><<<grid_for(n * width, 256), 256, 0, s>>>(coef.as<T>(), d_out, log_h, log_b,
-                                                                  width, ctab));
-  ZKB_CHECK_LAUNCH();
-  if (log_h > 0) {
-    const T *tw;
-    ZKB_TRY(get_twiddles<F>(log_h, false, &tw, s));
-    ZKB_TRY(run_passes<F>(d_out, d_out, log_h, width, 1ull << log_b, tw, false, (T)0, s));
+  if (log_h == 0) {
+    // a single row: every evaluation is the constant coefficient
+    ZKB_LAUNCH("lde_expand", s, lde_expand_kernel<F><<<grid_for(width, 256), 256, 0, s>>>(d_trace, d_out, 0, log_b, width, ctab));
+  } else {
+    const T *itw, *ftw;
+    ZKB_TRY(get_twiddles<F>(log_h, true, &itw, s));
+    ZKB_TRY(get_twiddles<F>(log_h, false, &ftw, s));
+    const std::vector<int> ks = plan_passes(log_h, pass_kmax<F>());
+    const int Kf = ks.back();
+    ScratchBuf coef;
+    const T *src = d_trace;
+    if (ks.size() > 1) {
+      ZKB_TRY(coef.alloc(n * width * sizeof(T), s));
+      std::vector<int> head(ks.begin(), ks.end() - 1);
+      ZKB_TRY(run_plan<F>(d_trace, coef.as<T>(), log_h, width, 1, itw, true, (T)0, head, log_h, s));
+      src = coef.as<T>();
+    }
+    const uint32_t Cf = width % 8 == 0 ? 8 : (width % 4 == 0 ? 4 : 1);
+    FusedGeom g;
+    g.L = log_h;
+    g.width = width;
+    g.chunks_per_row = width / Cf;
+    g.blocks = 1u << (log_h - Kf);
+    g.log_b = log_b;
+    g.n = n;
+    if ((uint64_t)g.chunks_per_row * g.blocks >= (1ull << 31)) {
+      set_error("LDE launch too large");
+      return ZKB_ERR_UNSUPPORTED;
+    }
+    ZKB_TRY(launch_fused_k<F>(Kf, src, d_out, g, itw, ftw, ctab, Cf, s));
+    std::vector<int> tail(ks.rbegin() + 1, ks.rend());
+    if (!tail.empty())
+      ZKB_TRY(run_plan<F>(d_out, d_out, log_h, width, 1ull << log_b, ftw, false, (T)0, tail,
+                          log_h - Kf, s));
   }
   if (!bitrev) {
     const int LN = log_h + log_b;
@@ -480,7 +732,6 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
     ScratchBuf tmp;
     ZKB_TRY(tmp.alloc(total * sizeof(T), s));
     ZKB_LAUNCH("bitrev_rows", s, bitrev_rows_kernel<F><<<grid_for(total, 256), 256, 0, s>>>(d_out, tmp.as<T>(), LN, width, total));
-    ZKB_CHECK_LAUNCH();
     ZKB_CHECK_CUDA(cudaMemcpyAsync(d_out, tmp.p, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
   }
   return ZKB_OK;
