@@ -1,19 +1,23 @@
 #!/usr/bin/env python
 """Benchmark of the polynomial-commitment hot path: trace cells/s committed.
 
-One step commits one synthetic trace the way TwoAdicFriPcs::commit does: coset
-LDE (blowup 2^log_blowup, shift = field generator), rows bit-reversed, Poseidon2
-MMCS over the rows (zkb_pcs_commit).  The default workload is BabyBear
-2^22 rows x 256 columns, blowup 2 — the 2^22 x 256 BabyBear LDE+commit named as
-the target shape; `--workload` selects the others.
+One step is one commitment job on a synthetic trace (zkb_pcs_commit_fri): coset LDE
+(blowup 2^log_blowup, shift = field generator) with rows bit-reversed, Poseidon2
+MMCS over the rows (TwoAdicFriPcs::commit), then for BabyBear the alpha-reduction of
+the committed columns into one F_p^4 codeword and the FRI commit phase on it (fold by
+2 down to 2^8 with a Merkle commit per layer, 100 query openings).  The default
+workload is BabyBear 2^22 rows x 256 columns, blowup 2 — the 2^22 x 256 BabyBear
+LDE+commit named as the target shape; `--workload` selects the others (Goldilocks
+jobs commit without the extension FRI phase).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 value : whole-job cells/s with the trace resident in HBM (CUDA events on the
         launching stream, max over ranks).
-e2e   : the same metric through the host-pointer call (zkb_pcs_commit) with the
-        trace in pinned host memory, its H2D copy and the root's D2H read inside
-        the timed region.
+e2e   : the same metric through the serving engine (zkb_engine_submit/wait, two
+        slots) with the trace in pinned host memory: every job's H2D copy and the
+        D2H read of its root and FRI answers are inside the timed region; one job's
+        copy overlaps another's kernels.
 --impl reference : the reference CPU path (restated in C, oracle/) on the host
         cores, on a bounded sample of the same workload.
 N > 1 runs one independent replica per GPU (torchrun; no data-path collective).
@@ -47,6 +51,8 @@ WORKLOADS = {
 DEFAULT_WORKLOAD = "babybear_2^22x256_b2"
 P2_SEED = 42
 TRACE_SEED = 20240607
+FRI = {"log_final": 8, "num_queries": 100, "challenge_seed": 7, "query_seed": 11}
+ALPHA = [123456789, 987654321, 55555, 4242]
 METRIC = "trace cells/s committed (LDE+Poseidon2 Merkle+FRI), batched vs plain; p99 ms"
 
 
@@ -118,8 +124,9 @@ class ClockSampler:
 
 # ------------------------------------------------------------ CPU legs
 def cpu_commit_sample(wl: dict, log_rows: int, threads: int) -> tuple[float, int]:
-    """Oracle (reference CPU path restated in C) LDE + MMCS commit of a
-    2^log_rows x width sample; returns (seconds, cells)."""
+    """Oracle (reference CPU path restated in C) commitment job — LDE + MMCS commit,
+    and for BabyBear the alpha-reduction + FRI commit phase — of a 2^log_rows x width
+    sample; returns (seconds, cells)."""
     import numpy as np
 
     import oracle as O
@@ -135,6 +142,11 @@ def cpu_commit_sample(wl: dict, log_rows: int, threads: int) -> tuple[float, int
     t0 = time.perf_counter()
     lde = O.coset_lde(wl["field"], t, wl["log_blowup"])
     O.mmcs_commit(h, [lde])
+    if wl["field"] == 0:
+        cw = O.combine_columns_ext4(lde, np.array(ALPHA, np.uint32))
+        log_n = log_rows + wl["log_blowup"]
+        O.fri_commit_ext4(cw, min(FRI["log_final"], log_n - 1), P2_SEED, FRI["challenge_seed"],
+                          FRI["num_queries"], FRI["query_seed"])
     return time.perf_counter() - t0, t.size
 
 
@@ -246,13 +258,30 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     pinned.copy_(trace)
     root = np.zeros(pcs.mmcs.digest_elems, dtype=np.uint32 if field == 0 else np.uint64)
     stream = torch.cuda.current_stream(dev)
+    with_fri = field == 0
+
+    def step_dev():
+        if with_fri:
+            _, _, pf = pcs.commit_fri_dev(trace, ALPHA, FRI["log_final"], FRI["num_queries"],
+                                          FRI["challenge_seed"], FRI["query_seed"], want_tree=False, root=root)
+            return pf.roots.copy()
+        pcs.commit_dev(trace, want_tree=False, root=root)
+        return None
+
+    engine = Z.CommitEngine(slots=2)
+    fri_desc = dict(FRI, alpha=ALPHA) if with_fri else None
+
+    def run_engine(k):
+        ids = [engine.submit(pinned, field=field, seed=P2_SEED, log_blowup=lb, p2_width=wl["p2w"], fri=fri_desc,
+                             host_ptr=pinned.data_ptr(), shape=(n, w)) for _ in range(k)]
+        return [engine.wait(j) for j in ids]
 
     # ---- warm-up (builds twiddle/coset tables, fills the memory pool)
     for _ in range(max(args.warmup, 1)):
-        pcs.commit_dev(trace, want_tree=False, root=root)
-    for _ in range(max(args.warmup, 1)):
-        pcs.commit_ptr(pinned.data_ptr(), n, w, want_tree=False, root=root)
+        fri_ref = step_dev()
     root_ref = root.copy()
+    warm = run_engine(max(args.warmup, 1))
+    assert all((r[0] == root_ref).all() for r in warm), "engine root differs from the device path"
 
     # ---- device-resident timed region (trace resident in HBM, > L2: no flush needed)
     sampler = ClockSampler(local_rank) if rank == 0 else None
@@ -264,7 +293,7 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        pcs.commit_dev(trace, want_tree=False, root=root)
+        fri_roots = step_dev()
     ev1.record(stream)
     ev1.synchronize()
     barrier()
@@ -272,16 +301,18 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     clocks = sampler.stop() if sampler else None
     t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     assert (root == root_ref).all(), "root changed between steps"
+    assert not with_fri or (fri_roots == fri_ref).all(), "FRI commitments changed between steps"
     gpu_launches = sum(v[0] for v in kstats.values())
 
-    # ---- end-to-end timed region (host pinned trace -> root on host, public host call)
+    # ---- end-to-end timed region: pinned host trace -> root and FRI answers on the host,
+    # through the serving engine (the copy of one job overlaps the kernels of another)
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        pcs.commit_ptr(pinned.data_ptr(), n, w, want_tree=False, root=root)
-    torch.cuda.synchronize()
+    res = run_engine(args.steps)
     t_e2e = max_over_ranks(time.perf_counter() - t0)
-    assert (root == root_ref).all()
+    assert all((r[0] == root_ref).all() for r in res)
+    e2e_lat = sorted(r[2]["latency_ms"] for r in res)
+    engine.close()
 
     # ---- integer-multiply ceiling for the Poseidon2 roofline (measured, this GPU)
     mul_peak = N.measure_mul_peak(field)
@@ -292,6 +323,9 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         return 0
 
     value = cells * args.steps * world / t_dev
+    rounds = wl["log_h"] + lb - FRI["log_final"]
+    fri_d2h = 4 * (8 * rounds + 4 * rounds + 4 * (1 << FRI["log_final"]) + FRI["num_queries"] * (
+        2 + 8 * rounds + 8 * sum(wl["log_h"] + lb - r - 1 for r in range(rounds))))
     e2e = cells * args.steps * world / t_e2e
     # roofline of the dominant kernel (leaf sponge hashing; integer-multiply bound)
     N_rows = n << lb
@@ -315,17 +349,29 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         hbm_peak, hbm_src = float(peaks["hbm_gbs"]), "of measured"
     except (OSError, ValueError, KeyError):
         hbm_peak, hbm_src = 6650.0, "of fallback"
+    # NTT kernels: plain passes read and write their tiles once; the fused kernel reads the
+    # coefficient matrix once and writes every coset block once
+    kmax = 11 if field == 0 else 10
+    n_pass = -(-wl["log_h"] // kmax)
+    b_blocks = 1 << lb
+    ntt_roof = []
     nk = kstats.get("ntt_pass")
-    ntt_roof = None
-    if nk:
-        n_inv_passes = (wl["log_h"] + 9) // 10
-        n_fwd_passes = n_inv_passes
-        bytes_per_step = 2 * esize * (n * w * n_inv_passes + N_rows * w * n_fwd_passes)
+    if nk and n_pass > 1:
+        bytes_per_step = 2 * esize * (n * w * (n_pass - 1) + N_rows * w * (n_pass - 1))
         per_launch = bytes_per_step * args.steps / nk[0]
         ach = per_launch / (nk[1] / nk[0] * 1e-3) / 1e9
-        ntt_roof = {"kernel": "ntt_pass", "bound": "hbm", "unit": "GB/s", "achieved": ach, "peak": hbm_peak,
-                    "frac": ach / hbm_peak, "peak_source": hbm_src,
-                    "traffic": traffic.get("ntt_pass") if traffic else None}
+        ntt_roof.append({"kernel": "ntt_pass", "bound": "hbm", "unit": "GB/s", "achieved": ach, "peak": hbm_peak,
+                         "frac": ach / hbm_peak, "peak_source": hbm_src,
+                         "algorithmic_bytes_per_launch": per_launch,
+                         "traffic": traffic.get("ntt_pass") if traffic else None})
+    fk = kstats.get("lde_fused")
+    if fk:
+        per_launch = esize * (n * w + b_blocks * n * w)
+        ach = per_launch / (fk[1] / fk[0] * 1e-3) / 1e9
+        ntt_roof.append({"kernel": "lde_fused", "bound": "hbm", "unit": "GB/s", "achieved": ach, "peak": hbm_peak,
+                         "frac": ach / hbm_peak, "peak_source": hbm_src,
+                         "algorithmic_bytes_per_launch": per_launch,
+                         "traffic": traffic.get("lde_fused") if traffic else None})
 
     # ---- CPU baseline (oracle on host cores, bounded sample)
     cpu = None
@@ -350,9 +396,13 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
                    "l2": "inputs larger than L2 (trace %.1f GB, LDE %.1f GB)" % (cells * esize / 1e9,
                                                                              N_rows * w * esize / 1e9)},
         "e2e": {"value": e2e, "unit": "cells/s", "h2d_bytes_per_step": cells * esize,
-                "d2h_bytes_per_step": int(root.nbytes), "ms_per_step": 1e3 * t_e2e / args.steps},
+                "d2h_bytes_per_step": int(root.nbytes) + (fri_d2h if with_fri else 0),
+                "ms_per_step": 1e3 * t_e2e / args.steps, "path": "zkb_engine_submit/wait, 2 slots",
+                "latency_ms_p50": e2e_lat[len(e2e_lat) // 2], "latency_ms_max": e2e_lat[-1]},
         "roofline": roofline,
         "roofline_ntt": ntt_roof,
+        "step": "LDE + Poseidon2 MMCS" + (" + alpha-reduction + FRI (2^%d -> 2^%d, %d queries)" % (
+            wl["log_h"] + lb, FRI["log_final"], FRI["num_queries"]) if with_fri else ""),
         "cpu_baseline": cpu,
         "gpu_launches": gpu_launches,
         "kernels": {k: {"launches": v[0], "ms_total": round(v[1], 3), "ms_max": round(v[2], 3)}

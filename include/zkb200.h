@@ -283,6 +283,45 @@ ZKB_API int zkb_pcs_commit_fri_dev(const zkb_hasher *hasher, const void *d_trace
                                    const zkb_fri_params *params, void *root_out, zkb_tree **tree_out,
                                    zkb_fri_proof **fri_out, void *stream);
 
+/* ---------------------------------------------------------------- serving */
+/* Continuous-batching engine for commit jobs (the role of the reference's proof-level
+ * scheduler, zkf-metal/src/batch_prover.rs:94-140, and its bounded in-flight pipeline,
+ * zkf-metal/src/pipeline.rs:23-126).  `slots` worker threads each own a stream; a
+ * queued job is admitted when its device-memory estimate fits the HBM budget (FIFO,
+ * later smaller jobs may pass a blocked head), runs with its LDE, trees and FRI layers
+ * device-resident, and releases its memory when its answers are on the host.  Jobs on
+ * different slots overlap on the GPU; a job's results depend only on its inputs. */
+typedef struct {
+  uint32_t slots;        /* concurrent jobs */
+  uint64_t hbm_budget;   /* bytes for job state; 0 = free device memory minus 2 GiB */
+} zkb_engine_config;
+typedef struct {
+  zkb_hasher hasher;
+  const void *trace;     /* host memory (pinned for full copy bandwidth), valid until done */
+  uint32_t log_h, width, log_blowup;
+  int with_fri;          /* BabyBear: alpha-reduction + FRI commit phase after the commit */
+  uint32_t alpha[4];
+  zkb_fri_params fri;    /* log_n is set from the trace */
+} zkb_job_desc;
+typedef struct {
+  int status;            /* ZKB_OK or the job's error */
+  uint32_t root[16];     /* OUT elements (u32 BabyBear; Goldilocks digests as 2 u32 each) */
+  double queue_ms, run_ms, latency_ms;
+} zkb_job_result;
+typedef struct {
+  uint64_t queued, completed, hbm_budget, hbm_in_use, hbm_peak;
+} zkb_engine_stats_t;
+typedef struct zkb_engine zkb_engine;
+ZKB_API int zkb_engine_create(const zkb_engine_config *config, zkb_engine **engine_out);
+/* Non-blocking; the descriptor is copied. */
+ZKB_API int zkb_engine_submit(zkb_engine *engine, const zkb_job_desc *job, uint64_t *job_id);
+/* Blocks until the job is done; fri_out (may be NULL) receives its FRI answers. */
+ZKB_API int zkb_engine_wait(zkb_engine *engine, uint64_t job_id, zkb_job_result *result,
+                            zkb_fri_proof **fri_out);
+ZKB_API int zkb_engine_stats(zkb_engine *engine, zkb_engine_stats_t *stats);
+/* Finishes the queued jobs, then stops the workers. */
+ZKB_API void zkb_engine_destroy(zkb_engine *engine);
+
 #ifdef __cplusplus
 }
 #endif

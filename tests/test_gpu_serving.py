@@ -1,0 +1,87 @@
+"""The continuous-batching engine: results are identical alone and in the mix.
+
+Jobs of mixed sizes (both fields, with and without the FRI phase) run first one at a
+time on a one-slot engine, then all submitted at once to a four-slot engine where they
+overlap on the GPU; every root, FRI commitment, final codeword and query answer must
+match bit for bit (tolerance 0), and match the oracle for the small ones."""
+import numpy as np
+import pytest
+
+import ziros_b200 as Z
+from conftest import rand_field
+
+pytestmark = pytest.mark.gpu
+
+
+def _jobs():
+    jobs = []
+    for k, (field, log_h, w) in enumerate([(0, 12, 16), (0, 14, 40), (1, 10, 24), (0, 16, 64), (0, 9, 8),
+                                           (1, 13, 8), (0, 15, 128), (0, 11, 256)]):
+        trace = rand_field(field, (1 << log_h, w), 900 + k)
+        fri = None
+        if field == 0 and k % 2 == 0:
+            fri = {"alpha": rand_field(0, 4, 950 + k), "log_final": 3, "num_queries": 7,
+                   "challenge_seed": 17 + k, "query_seed": 23 + k}
+        jobs.append((field, trace, fri))
+    return jobs
+
+
+def _run(engine, jobs, concurrent):
+    out = [None] * len(jobs)
+    if concurrent:
+        ids = [engine.submit(t, field=f, seed=42, log_blowup=1, fri=fr) for f, t, fr in jobs]
+        for i, jid in enumerate(ids):
+            out[i] = engine.wait(jid)
+    else:
+        for i, (f, t, fr) in enumerate(jobs):
+            out[i] = engine.wait(engine.submit(t, field=f, seed=42, log_blowup=1, fri=fr))
+    return out
+
+
+def test_results_identical_alone_and_in_the_mix(oracle):
+    jobs = _jobs()
+    solo = Z.CommitEngine(slots=1)
+    alone = _run(solo, jobs, concurrent=False)
+    solo.close()
+    eng = Z.CommitEngine(slots=4)
+    mixed = _run(eng, jobs, concurrent=True)
+    st = eng.stats()
+    eng.close()
+    assert st["completed"] == len(jobs) and st["hbm_peak"] <= st["hbm_budget"]
+    for (field, trace, fri), a, m in zip(jobs, alone, mixed):
+        assert (a[0] == m[0]).all()
+        if fri:
+            assert (a[1].roots == m[1].roots).all() and (a[1].final == m[1].final).all()
+            assert (a[1].query_rows == m[1].query_rows).all()
+            assert (a[1].query_siblings == m[1].query_siblings).all()
+        else:
+            assert a[1] is None and m[1] is None
+    # small jobs against the oracle
+    for (field, trace, fri), a in zip(jobs, alone):
+        if trace.shape[0] <= 1 << 12:
+            lde = oracle.coset_lde(field, trace, 1)
+            layers = oracle.mmcs_commit(oracle.hasher(field, 42), [lde])
+            assert (a[0] == layers[-1][0]).all()
+
+
+def test_admission_by_hbm_budget():
+    """A budget that fits one job at a time still completes every job correctly."""
+    jobs = [(0, rand_field(0, (1 << 14, 32), 60 + k), None) for k in range(4)]
+    ref = Z.CommitEngine(slots=1)
+    want = _run(ref, jobs, concurrent=False)
+    ref.close()
+    per_job = (1 << 14) * 32 * 4 * 4 + (64 << 20)
+    eng = Z.CommitEngine(slots=4, hbm_budget=int(per_job * 1.5))
+    got = _run(eng, jobs, concurrent=True)
+    st = eng.stats()
+    eng.close()
+    assert st["hbm_peak"] <= st["hbm_budget"]
+    for a, b in zip(want, got):
+        assert (a[0] == b[0]).all()
+
+
+def test_rejects_job_larger_than_budget():
+    eng = Z.CommitEngine(slots=1, hbm_budget=1 << 20)
+    with pytest.raises(Z.ZkbError):
+        eng.submit(rand_field(0, (1 << 12, 16), 1))
+    eng.close()

@@ -56,6 +56,26 @@ class FriParams(C.Structure):
                 ("num_queries", C.c_uint32), ("query_seed", C.c_uint64)]
 
 
+class EngineConfig(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("hbm_budget", C.c_uint64)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("hasher", Hasher), ("trace", C.c_void_p), ("log_h", C.c_uint32), ("width", C.c_uint32),
+                ("log_blowup", C.c_uint32), ("with_fri", C.c_int), ("alpha", C.c_uint32 * 4),
+                ("fri", FriParams)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("root", C.c_uint32 * 16), ("queue_ms", C.c_double),
+                ("run_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
+class EngineStats(C.Structure):
+    _fields_ = [("queued", C.c_uint64), ("completed", C.c_uint64), ("hbm_budget", C.c_uint64),
+                ("hbm_in_use", C.c_uint64), ("hbm_peak", C.c_uint64)]
+
+
 # Every symbol of include/zkb200.h with its ctypes signature.
 _P = C.c_void_p
 _SZ = C.c_size_t
@@ -105,6 +125,11 @@ SIGNATURES = {
     "zkb_fri_proof_free": (None, [_P]),
     "zkb_combine_columns_babybear_ext4_dev": (_I, [_P, _U64, _U32, _P, _P, _P]),
     "zkb_pcs_commit_fri": (_I, [_P, _P, _U32, _U32, _U32, _P, _P, _P, _P, _P]),
+    "zkb_engine_create": (_I, [_P, _P]),
+    "zkb_engine_submit": (_I, [_P, _P, _P]),
+    "zkb_engine_wait": (_I, [_P, _U64, _P, _P]),
+    "zkb_engine_stats": (_I, [_P, _P]),
+    "zkb_engine_destroy": (None, [_P]),
     "zkb_pcs_commit_fri_dev": (_I, [_P, _P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P]),
 }
 

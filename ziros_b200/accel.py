@@ -379,6 +379,8 @@ class FriProof:
         self._h = handle
         self.log_n, self.log_final = params.log_n, params.log_final
         self.rounds = lib.zkb_fri_num_rounds(handle)
+        if self.rounds != self.log_n - self.log_final:
+            raise N.ZkbError(f"FRI proof has {self.rounds} rounds, expected {self.log_n - self.log_final}")
         self.roots = np.zeros((self.rounds, 8), np.uint32)
         self.betas = np.zeros((self.rounds, 4), np.uint32)
         N.check(lib.zkb_fri_commitments(handle, _ptr(self.roots), _ptr(self.betas)))
@@ -447,3 +449,66 @@ def combine_columns_dev(lde, alpha, out) -> None:
     lp, stream = _torch_ptr_stream(lde)
     op, _ = _torch_ptr_stream(out)
     N.check(N.load().zkb_combine_columns_babybear_ext4_dev(lp, lde.shape[0], lde.shape[1], _ptr(a), op, stream))
+
+
+class CommitEngine:
+    """Continuous-batching commit engine (zkb_engine_*): jobs are submitted without
+    blocking, admitted by free HBM and slot, and overlap on the device."""
+
+    def __init__(self, slots: int = 2, hbm_budget: int = 0):
+        lib = N.load()
+        self._h = C.c_void_p()
+        N.check(lib.zkb_engine_create(C.byref(N.EngineConfig(slots, hbm_budget)), C.byref(self._h)))
+        self._keep = {}
+
+    def submit(self, trace, field: int = BABYBEAR, seed: int = 42, log_blowup: int = 1, p2_width: int = 16,
+               fri: Optional[dict] = None, host_ptr: Optional[int] = None, shape=None) -> int:
+        """trace: host array (kept alive until the job is waited on), or host_ptr + shape."""
+        if host_ptr is None:
+            t = np.ascontiguousarray(trace, dtype=dtype_of(field))
+            ptr, (h, w) = t.ctypes.data, t.shape
+        else:
+            t, ptr, (h, w) = trace, host_ptr, shape
+        d = N.JobDesc()
+        d.hasher = N.Hasher(field, p2_width, seed)
+        d.trace = ptr
+        d.log_h, d.width, d.log_blowup = h.bit_length() - 1, w, log_blowup
+        if fri:
+            d.with_fri = 1
+            d.alpha[:] = [int(x) for x in fri["alpha"]]
+            d.fri = N.FriParams(0, fri["log_final"], fri["challenge_seed"], fri["num_queries"], fri["query_seed"])
+        jid = C.c_uint64()
+        N.check(N.load().zkb_engine_submit(self._h, C.byref(d), C.byref(jid)))
+        self._keep[jid.value] = (t, d)
+        return jid.value
+
+    def wait(self, job_id: int):
+        """-> (root, FriProof or None, {queue_ms, run_ms, latency_ms})"""
+        res = N.JobResult()
+        fh = C.c_void_p()
+        rc = N.load().zkb_engine_wait(self._h, job_id, C.byref(res), C.byref(fh))
+        _, d = self._keep.pop(job_id)
+        N.check(rc)
+        field = d.hasher.field
+        out = 8 if d.hasher.width == 16 else 4
+        raw = np.array(res.root[:], dtype=np.uint32)
+        root = raw[:out] if field == BABYBEAR else raw.view(np.uint64)[:out]
+        pf = None
+        if fh:
+            prm = N.FriParams(d.log_h + d.log_blowup, d.fri.log_final, d.fri.challenge_seed, d.fri.num_queries,
+                              d.fri.query_seed)
+            pf = FriProof(fh, prm)
+        return root, pf, {"queue_ms": res.queue_ms, "run_ms": res.run_ms, "latency_ms": res.latency_ms}
+
+    def stats(self) -> dict:
+        st = N.EngineStats()
+        N.check(N.load().zkb_engine_stats(self._h, C.byref(st)))
+        return {k: int(getattr(st, k)) for k, _ in N.EngineStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.load().zkb_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -1,4 +1,6 @@
 // abi.cu — extern "C" entry points declared in include/zkb200.h.
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -13,13 +15,7 @@ int measure_mul_peak(int field, double *mul_per_s);
 
 using namespace zkb;
 
-struct zkb_tree {
-  DeviceTree t;
-};
 
-struct zkb_fri_proof {
-  FriProof f;
-};
 
 namespace {
 
@@ -310,7 +306,7 @@ namespace {
 int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_trace, uint32_t log_h,
                     uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out,
                     cudaStream_t s, const uint32_t *alpha = nullptr, const zkb_fri_params *fri = nullptr,
-                    zkb_fri_proof **fri_out = nullptr) {
+                    FriProof *fri_out = nullptr) {
   ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
   const size_t es = field_elem_bytes(spec.field);
   const uint64_t n = 1ull << log_h, N = n << log_blowup;
@@ -338,21 +334,36 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
   ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));
   if (fri) {
     // alpha-reduction of the committed columns, then the FRI commit phase on it
+    ZKB_REQUIRE(fri_out != nullptr, "internal: FRI job without a proof object");
     const int log_n = (int)(log_h + log_blowup);
     void *cw = nullptr;
     ZKB_TRY(dev_alloc(&cw, N * 16, s));
-    auto pf = std::make_unique<zkb_fri_proof>();
-    pf->f.owned.push_back(cw);
-    pf->f.stream = s;
-    ZKB_CHECK_CUDA(cudaGetDevice(&pf->f.device));
+    fri_out->owned.push_back(cw);
+    fri_out->stream = s;
+    ZKB_CHECK_CUDA(cudaGetDevice(&fri_out->device));
     ZKB_TRY(combine_columns_ext4_dev((const uint32_t *)lde, N, width, alpha, (uint32_t *)cw, s));
     ZKB_TRY(fri_commit_ext4_dev(spec, (const uint32_t *)cw, log_n, (int)fri->log_final,
-                                fri->challenge_seed, (int)fri->num_queries, fri->query_seed, &pf->f, s));
-    if (fri_out) *fri_out = pf.release();
+                                fri->challenge_seed, (int)fri->num_queries, fri->query_seed, fri_out, s));
   }
   return tree_from(tree_out, tree, root_out, s);
 }
 }  // namespace
+
+}  // extern "C"
+
+// One engine job: host trace in, root (and the FRI answers) out, device state released
+// before returning.
+int zkb::pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
+                     uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
+                     FriProof *fri_out, cudaStream_t s) {
+  int rc = pcs_commit_impl(spec, nullptr, h_trace, log_h, width, log_blowup, root_out, nullptr, s,
+                           alpha, fri, fri_out);
+  if (fri_out) fri_out->release_device();
+  if (rc == ZKB_OK) ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  return rc;
+}
+
+extern "C" {
 
 int zkb_pcs_commit(const zkb_hasher *hasher, const void *trace, uint32_t log_h, uint32_t width,
                    uint32_t log_blowup, void *root_out, zkb_tree **tree_out) {
@@ -382,8 +393,11 @@ int zkb_pcs_commit_fri(const zkb_hasher *hasher, const void *trace, uint32_t log
   ZKB_TRY(hasher_spec(hasher, &spec));
   ZKB_REQUIRE(spec.field == FIELD_BABYBEAR, "the FRI job runs over the BabyBear quartic extension");
   ZKB_REQUIRE(trace != nullptr && width > 0 && alpha != nullptr && params != nullptr, "bad arguments");
-  return pcs_commit_impl(spec, nullptr, trace, log_h, width, log_blowup, root_out, tree_out,
-                         thread_stream(), alpha, params, fri_out);
+  auto pf = std::make_unique<zkb_fri_proof>();
+  ZKB_TRY(pcs_commit_impl(spec, nullptr, trace, log_h, width, log_blowup, root_out, tree_out,
+                          thread_stream(), alpha, params, &pf->f));
+  if (fri_out) *fri_out = pf.release();
+  return ZKB_OK;
 }
 
 int zkb_pcs_commit_fri_dev(const zkb_hasher *hasher, const void *d_trace, uint32_t log_h, uint32_t width,
@@ -394,8 +408,11 @@ int zkb_pcs_commit_fri_dev(const zkb_hasher *hasher, const void *d_trace, uint32
   ZKB_TRY(hasher_spec(hasher, &spec));
   ZKB_REQUIRE(spec.field == FIELD_BABYBEAR, "the FRI job runs over the BabyBear quartic extension");
   ZKB_REQUIRE(d_trace != nullptr && width > 0 && alpha != nullptr && params != nullptr, "bad arguments");
-  return pcs_commit_impl(spec, d_trace, nullptr, log_h, width, log_blowup, root_out, tree_out,
-                         resolve_stream(stream), alpha, params, fri_out);
+  auto pf = std::make_unique<zkb_fri_proof>();
+  ZKB_TRY(pcs_commit_impl(spec, d_trace, nullptr, log_h, width, log_blowup, root_out, tree_out,
+                          resolve_stream(stream), alpha, params, &pf->f));
+  if (fri_out) *fri_out = pf.release();
+  return ZKB_OK;
 }
 
 const void *zkb_tree_matrix_dev(const zkb_tree *tree, int mat) {
@@ -538,7 +555,8 @@ int zkb_fri_commit_babybear_ext4(const zkb_hasher *hasher, const zkb_fri_params 
 
 int zkb_fri_num_rounds(const zkb_fri_proof *p) {
   if (!p) return ZKB_ERR_INVALID;
-  return (int)p->f.trees.size();
+  // counted from the host answers: the device trees may already have been released
+  return (int)p->f.betas.size();
 }
 
 int zkb_fri_commitments(const zkb_fri_proof *p, uint32_t *roots_out, uint32_t *betas_out) {

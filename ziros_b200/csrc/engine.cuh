@@ -57,8 +57,9 @@ struct DeviceTree {
 };
 
 // p3 MerkleTree::new over device matrices; fills layers and the tree description.
+// fri_layer only renames the kernels for the timing hook (fri_leaf_hash / fri_compress).
 int mmcs_build_dev(const HasherSpec &h, const std::vector<TreeMatrix> &mats, DeviceTree *tree,
-                   cudaStream_t s);
+                   cudaStream_t s, bool fri_layer = false);
 // Copy the root (spec.out elements) to host memory (synchronises the stream).
 int mmcs_root_to_host(const DeviceTree *tree, void *root_out, cudaStream_t s);
 
@@ -83,8 +84,15 @@ struct FriProof {
   std::vector<uint32_t> query_rows;                // queries x rounds x 8
   std::vector<uint32_t> query_sibs;                // queries x sib_per_query
   uint64_t sib_per_query = 0;
+  // Frees the device buffers (trees, folded codewords); host answers stay.
+  void release_device();
   ~FriProof();
 };
+
+// One PCS commit job from host memory (+ FRI when `fri` is set), device state released.
+int pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
+                uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
+                FriProof *fri_out, cudaStream_t s);
 int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
                              const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s);
 int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int log_n, int log_final,
@@ -92,3 +100,12 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
                         FriProof *pf, cudaStream_t s);
 
 }  // namespace zkb
+
+// Opaque handles of the C ABI.
+struct zkb_tree {
+  zkb::DeviceTree t;
+};
+
+struct zkb_fri_proof {
+  zkb::FriProof f;
+};

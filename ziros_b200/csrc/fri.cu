@@ -208,14 +208,17 @@ __global__ void fri_gather_kernel(const FriRoundDesc *__restrict__ rounds, int n
   }
 }
 
-FriProof::~FriProof() {
+void FriProof::release_device() {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
   trees.clear();
   for (void *p : owned) cudaFreeAsync(p, stream);
+  owned.clear();
   cudaSetDevice(prev);
 }
+
+FriProof::~FriProof() { release_device(); }
 
 int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int log_n, int log_final,
                         uint64_t challenge_seed, int num_queries, uint64_t query_seed,
@@ -237,7 +240,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
   for (int r = 0; r < rounds; r++) {
     auto tree = std::make_unique<DeviceTree>();
     std::vector<TreeMatrix> m{{cur, len / 2, 8}};
-    ZKB_TRY(mmcs_build_dev(spec, m, tree.get(), s));
+    ZKB_TRY(mmcs_build_dev(spec, m, tree.get(), s, true));
     std::array<uint32_t, 4> beta;
     for (auto &b : beta) b = sample_babybear(rng);
     pf->betas.push_back(beta);

@@ -128,7 +128,9 @@ static int log2_ceil(uint64_t x) {
 
 template <class F, int W>
 static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &mats,
-                           DeviceTree *t, cudaStream_t s) {
+                           DeviceTree *t, cudaStream_t s, bool fri_layer) {
+  const char *leaf_name = fri_layer ? "fri_leaf_hash" : "merkle_leaf_hash";
+  const char *comp_name = fri_layer ? "fri_compress" : "merkle_compress";
   using T = typename F::T;
   constexpr int OUT = p2_out<W>();
   P2Params<F, W> p;
@@ -200,7 +202,7 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
   ZKB_TRY(make_list(0, ng, &ml));
   const unsigned thr = 128;
   const unsigned cap = (unsigned)ctx->sm_count * 16u;
-  ZKB_LAUNCH("merkle_leaf_hash", s, hash_rows_kernel<F, W><<<grid_for(max_h, thr, cap), thr, 0, s>>>(ml, max_h, layers, p));
+  ZKB_LAUNCH(leaf_name, s, hash_rows_kernel<F, W><<<grid_for(max_h, thr, cap), thr, 0, s>>>(ml, max_h, layers, p));
   ZKB_CHECK_LAUNCH();
   ScratchBuf inj_buf;  // digests of rows injected at one layer (sized for the largest)
 
@@ -225,18 +227,18 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
       inj = inj_buf.as<T>();
     }
     next_m += ni;
-    ZKB_LAUNCH("merkle_compress", s, compress_kernel<F, W><<<grid_for(half, thr, cap), thr, 0, s>>>(prev, next, half, inj, inj_h, p));
+    ZKB_LAUNCH(comp_name, s, compress_kernel<F, W><<<grid_for(half, thr, cap), thr, 0, s>>>(prev, next, half, inj, inj_h, p));
     ZKB_CHECK_LAUNCH();
   }
   return ZKB_OK;
 }
 
 int mmcs_build_dev(const HasherSpec &h, const std::vector<TreeMatrix> &mats, DeviceTree *tree,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool fri_layer) {
   ZKB_REQUIRE(!mats.empty(), "No matrices given");
-  if (h.field == FIELD_BABYBEAR && h.width == 16) return build_tree_impl<BabyBear, 16>(h, mats, tree, s);
-  if (h.field == FIELD_GOLDILOCKS && h.width == 16) return build_tree_impl<Goldilocks, 16>(h, mats, tree, s);
-  if (h.field == FIELD_GOLDILOCKS && h.width == 12) return build_tree_impl<Goldilocks, 12>(h, mats, tree, s);
+  if (h.field == FIELD_BABYBEAR && h.width == 16) return build_tree_impl<BabyBear, 16>(h, mats, tree, s, fri_layer);
+  if (h.field == FIELD_GOLDILOCKS && h.width == 16) return build_tree_impl<Goldilocks, 16>(h, mats, tree, s, fri_layer);
+  if (h.field == FIELD_GOLDILOCKS && h.width == 12) return build_tree_impl<Goldilocks, 12>(h, mats, tree, s, fri_layer);
   set_error("unsupported hasher: field %d width %d", h.field, h.width);
   return ZKB_ERR_UNSUPPORTED;
 }
