@@ -14,7 +14,7 @@ jobs commit without the extension FRI phase).
 
 value : whole-job cells/s with the trace resident in HBM (CUDA events on the
         launching stream, max over ranks).
-e2e   : the same metric through the serving engine (zkb_engine_submit/wait, two
+e2e   : the same metric through the serving engine (zkb_engine_submit/wait, three
         slots) with the trace in pinned host memory: every job's H2D copy and the
         D2H read of its root and FRI answers are inside the timed region; one job's
         copy overlaps another's kernels.
@@ -53,6 +53,7 @@ P2_SEED = 42
 TRACE_SEED = 20240607
 FRI = {"log_final": 8, "num_queries": 100, "challenge_seed": 7, "query_seed": 11}
 ALPHA = [123456789, 987654321, 55555, 4242]
+E2E_SLOTS = 3  # engine slots of the e2e leg: a job's H2D copy overlaps two others' kernels
 METRIC = "trace cells/s committed (LDE+Poseidon2 Merkle+FRI), batched vs plain; p99 ms"
 
 
@@ -268,7 +269,7 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         pcs.commit_dev(trace, want_tree=False, root=root)
         return None
 
-    engine = Z.CommitEngine(slots=2)
+    engine = Z.CommitEngine(slots=E2E_SLOTS)
     fri_desc = dict(FRI, alpha=ALPHA) if with_fri else None
 
     def run_engine(k):
@@ -397,7 +398,7 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
                                                                              N_rows * w * esize / 1e9)},
         "e2e": {"value": e2e, "unit": "cells/s", "h2d_bytes_per_step": cells * esize,
                 "d2h_bytes_per_step": int(root.nbytes) + (fri_d2h if with_fri else 0),
-                "ms_per_step": 1e3 * t_e2e / args.steps, "path": "zkb_engine_submit/wait, 2 slots",
+                "ms_per_step": 1e3 * t_e2e / args.steps, "path": f"zkb_engine_submit/wait, {E2E_SLOTS} slots",
                 "latency_ms_p50": e2e_lat[len(e2e_lat) // 2], "latency_ms_max": e2e_lat[-1]},
         "roofline": roofline,
         "roofline_ntt": ntt_roof,

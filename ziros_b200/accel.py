@@ -171,9 +171,12 @@ class Tree:
 
     def __del__(self):
         h = getattr(self, "_h", None)
+        self._h = None
         if h:
-            N.load().zkb_tree_free(h)
-            self._h = None
+            try:
+                N.load().zkb_tree_free(h)
+            except Exception:  # interpreter shutdown: module state already torn down
+                pass
 
     @property
     def digest_elems(self) -> int:
@@ -397,9 +400,12 @@ class FriProof:
 
     def __del__(self):
         h = getattr(self, "_h", None)
+        self._h = None
         if h:
-            N.load().zkb_fri_proof_free(h)
-            self._h = None
+            try:
+                N.load().zkb_fri_proof_free(h)
+            except Exception:  # interpreter shutdown: module state already torn down
+                pass
 
     def siblings(self, q: int, r: int) -> np.ndarray:
         """Sibling digests of query q in round r: (log_n - r - 1, 8)."""

@@ -51,6 +51,11 @@ struct BabyBear {
     uint64_t u = t + (uint64_t)m * P;
     return (uint32_t)(u >> 32);
   }
+  // t * 2^-32 mod p, canonical, for any t < p*2^32 (e.g. a sum of mont_lazy results).
+  __host__ __device__ __forceinline__ static uint32_t mont_reduce(uint64_t t) {
+    uint32_t m = (uint32_t)t * NPINV;
+    return red((uint32_t)((t + (uint64_t)m * P) >> 32));
+  }
   // Fully reduced Montgomery product (both operands < p).
   __host__ __device__ __forceinline__ static uint32_t mont(uint32_t a, uint32_t b) {
     return red(mont_lazy(a, b));

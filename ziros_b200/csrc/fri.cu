@@ -307,18 +307,22 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
 
 namespace zkb {
 
-// out[i] = sum_j alpha^j * lde[i][j] over BabyBear^4.  alpha powers are Montgomery-encoded
-// coefficientwise (a base x extension product is four Montgomery products); the four
-// running sums stay unreduced in 64 bits and are reduced once per row.
+// out[i] = sum_j alpha^j * lde[i][j] over BabyBear^4.  One warp per row: lane l reads
+// columns l, l+32, ... (coalesced), so a warp streams whole rows.  The powers arrive
+// encoded as alpha^j * 2^64 mod p, so each Montgomery product is v * alpha^j * 2^32 and
+// a lane's unreduced 64-bit sum (below p * 2^32 for any width < 2^30) needs one
+// Montgomery reduction to come out as sum v * alpha^j; the 32 lane sums are then added
+// mod p across the warp.
 __global__ void __launch_bounds__(256)
     combine_columns_kernel(const uint32_t *__restrict__ lde, uint64_t rows, uint32_t width,
                            const uint4 *__restrict__ apow, uint4 *__restrict__ out) {
   using B = BabyBear;
-  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows;
-       r += (uint64_t)gridDim.x * blockDim.x) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
     const uint32_t *row = lde + r * width;
     uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-    for (uint32_t j = 0; j < width; j++) {
+    for (uint32_t j = lane; j < width; j += 32) {
       const uint32_t v = row[j];
       const uint4 w = apow[j];
       a0 += B::mont_lazy(v, w.x);
@@ -326,8 +330,16 @@ __global__ void __launch_bounds__(256)
       a2 += B::mont_lazy(v, w.z);
       a3 += B::mont_lazy(v, w.w);
     }
-    out[r] = make_uint4((uint32_t)(a0 % B::P), (uint32_t)(a1 % B::P), (uint32_t)(a2 % B::P),
-                        (uint32_t)(a3 % B::P));
+    uint32_t c0 = B::mont_reduce(a0), c1 = B::mont_reduce(a1), c2 = B::mont_reduce(a2),
+             c3 = B::mont_reduce(a3);
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+      c0 = B::add(c0, __shfl_xor_sync(0xffffffffu, c0, off));
+      c1 = B::add(c1, __shfl_xor_sync(0xffffffffu, c1, off));
+      c2 = B::add(c2, __shfl_xor_sync(0xffffffffu, c2, off));
+      c3 = B::add(c3, __shfl_xor_sync(0xffffffffu, c3, off));
+    }
+    if (lane == 0) out[r] = make_uint4(c0, c1, c2, c3);
   }
 }
 
@@ -345,7 +357,7 @@ int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t widt
   std::vector<uint32_t> pw((size_t)width * 4);
   uint32_t cur[4] = {1, 0, 0, 0};
   for (uint32_t j = 0; j < width; j++) {
-    for (int k = 0; k < 4; k++) pw[j * 4 + k] = BabyBear::tw_encode(cur[k]);
+    for (int k = 0; k < 4; k++) pw[j * 4 + k] = BabyBear::tw_encode(BabyBear::tw_encode(cur[k]));
     uint32_t nx[4];
     ext4_mul_host(cur, alpha, nx);
     for (int k = 0; k < 4; k++) cur[k] = nx[k];
@@ -355,7 +367,8 @@ int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t widt
   ZKB_CHECK_CUDA(cudaMemcpyAsync(d_pw.p, pw.data(), pw.size() * 4, cudaMemcpyHostToDevice, s));
   DeviceContext *ctx;
   ZKB_TRY(current_context(&ctx));
-  ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<<<grid_for(rows, 256, (unsigned)ctx->sm_count * 8u), 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
+  ZKB_REQUIRE(width < (1u << 30), "width too large");
+  ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<<<grid_for(rows * 32, 256, (unsigned)ctx->sm_count * 8u), 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
   // the host copy of the powers must outlive the asynchronous upload
   ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
   return ZKB_OK;
