@@ -47,6 +47,9 @@ WORKLOADS = {
     "babybear_2^14x16_b2": dict(field=0, log_h=14, width=16, log_blowup=1, p2w=16),
     # a smaller case of the default workload for profiler captures (inputs still > L2)
     "babybear_2^18x256_b2": dict(field=0, log_h=18, width=256, log_blowup=1, p2w=16),
+    # batched form: 64 traces, log2 rows uniform in [12, 22], widths uniform in {8, ..., 256}
+    "batch64_babybear": dict(kind="batch", field=0, n=64, log_h_lo=12, log_h_hi=22, w_step=8, w_hi=256,
+                             log_blowup=1, p2w=16, seed=4, width=128, log_h=22),
 }
 DEFAULT_WORKLOAD = "babybear_2^22x256_b2"
 P2_SEED = 42
@@ -143,7 +146,7 @@ def cpu_commit_sample(wl: dict, log_rows: int, threads: int) -> tuple[float, int
     t0 = time.perf_counter()
     lde = O.coset_lde(wl["field"], t, wl["log_blowup"])
     O.mmcs_commit(h, [lde])
-    if wl["field"] == 0:
+    if wl["field"] == 0 and wl.get("kind") != "batch":
         cw = O.combine_columns_ext4(lde, np.array(ALPHA, np.uint32))
         log_n = log_rows + wl["log_blowup"]
         O.fri_commit_ext4(cw, min(FRI["log_final"], log_n - 1), P2_SEED, FRI["challenge_seed"],
@@ -208,6 +211,23 @@ def make_trace(torch, wl: dict, device):
     eps = (1 << 32) - 1
     big = (v < 0) & (v >= -(1 << 32) + 1)
     return torch.where(big, v + eps, v)
+
+
+def batch_shapes(wl: dict) -> list:
+    import numpy as np
+
+    rng = np.random.default_rng(wl["seed"])
+    lh = rng.integers(wl["log_h_lo"], wl["log_h_hi"] + 1, size=wl["n"])
+    ws = wl["w_step"] * rng.integers(1, wl["w_hi"] // wl["w_step"] + 1, size=wl["n"])
+    return [(1 << int(a), int(b)) for a, b in zip(lh, ws)]
+
+
+def fill_uniform(torch, field: int, shape, seed: int, device):
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    if field == 0:
+        return torch.randint(0, BB_P, shape, dtype=torch.int32, device=device, generator=g)
+    return make_trace(torch, {"field": 1, "log_h": shape[0].bit_length() - 1, "width": shape[1]}, device)
 
 
 def load_traffic(workload: str):
@@ -416,6 +436,193 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     return 0
 
 
+def run_batch(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
+    """Batched form: 64 uneven BabyBear traces committed by one plan (one CUDA graph per
+    step, autotuned kernel shapes) against the plain path (64 zkb_pcs_commit_dev calls)
+    on the same GPU and the same device-resident traces."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import ziros_b200 as Z
+    from ziros_b200 import _native as N
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = N.load()
+    N.check(lib.zkb_set_device(local_rank))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    field, lb, p2w = wl["field"], wl["log_blowup"], wl["p2w"]
+    shapes = batch_shapes(wl)
+    cells = sum(h * w for h, w in shapes)
+    esize = 4 if field == 0 else 8
+    stream = torch.cuda.current_stream(dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    t0 = time.perf_counter()
+    batch = Z.BatchCommit(shapes, field=field, seed=P2_SEED, log_blowup=lb, p2_width=p2w, use_graph=True,
+                          autotune=True)
+    create_s = time.perf_counter() - t0
+    info = batch.info()
+    # traces generated on the device straight into the plan's input buffers
+    ptrs = []
+    for i, (h, w) in enumerate(shapes):
+        t = fill_uniform(torch, field, (h, w), TRACE_SEED + i, dev)
+        batch.copy_in(i, t)
+        p = C.c_void_p()
+        N.check(lib.zkb_batch_trace_ptr(batch._h, i, C.byref(p)))
+        ptrs.append(p)
+        del t
+    torch.cuda.synchronize()
+    hasher = N.Hasher(field, p2w, P2_SEED)
+    digest = 8 if p2w == 16 else 4
+    dt = np.uint32 if field == 0 else np.uint64
+    plain_roots = np.zeros((len(shapes), digest), dtype=dt)
+
+    def plain_step():
+        for i, (h, w) in enumerate(shapes):
+            N.check(lib.zkb_pcs_commit_dev(C.byref(hasher), ptrs[i], h.bit_length() - 1, w, lb,
+                                           plain_roots[i].ctypes.data_as(C.c_void_p), None, sp))
+
+    def batch_step():
+        batch.run(sp)
+
+    def timed(fn, k):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3)
+
+    for _ in range(max(args.warmup, 1)):
+        plain_step()
+        batch_step()
+    got = batch.roots(sp)
+    assert (got == plain_roots).all(), "batched roots differ from the plain per-trace commits"
+
+    N.profile_start()
+    t_plain = timed(plain_step, args.steps)
+    kstats = N.profile_stop()
+    plain_launches = sum(v[0] for v in kstats.values())
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.4)
+    t_batch = timed(batch_step, args.steps)
+    clocks = sampler.stop() if sampler else None
+    assert (batch.roots(sp) == plain_roots).all()
+
+    # end to end: traces from pinned host memory (one pinned buffer of the largest trace
+    # serves every trace), H2D copies + run + root read-back inside the timed region
+    hmax = max(h * w for h, w in shapes)
+    pinned = torch.empty(hmax, dtype=torch.int32 if field == 0 else torch.int64).pin_memory()
+    pinned.copy_(fill_uniform(torch, field, (hmax, 1), TRACE_SEED, dev).view(-1).cpu())
+
+    def e2e_step():
+        for i, (h, w) in enumerate(shapes):
+            N.check(lib.zkb_batch_copy_in(batch._h, i, C.c_void_p(pinned.data_ptr()), 0, sp))
+        batch.run(sp)
+        return batch.roots(sp)
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    # the plain path end to end: 64 host-pointer commits
+    pcs = Z.CudaTwoAdicPcs(field, P2_SEED, lb, p2w)
+    r = np.zeros(digest, dtype=dt)
+    pcs.commit_ptr(pinned.data_ptr(), shapes[0][0], shapes[0][1], want_tree=False, root=r)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for h, w in shapes:
+            pcs.commit_ptr(pinned.data_ptr(), h, w, want_tree=False, root=r)
+    t_e2e_plain = max_over_ranks(time.perf_counter() - t0)
+
+    mul_peak = N.measure_mul_peak(field)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    muls = 0
+    for h, w in shapes:
+        lp, cp = perms_of_commit((h << lb).bit_length() - 1, w)
+        muls += (lp + cp) * p2_field_muls(field, p2w)
+    value = cells * args.steps * world / t_batch
+    plain = cells * args.steps * world / t_plain
+    ach = muls * args.steps / t_batch / 1e9
+    cpu = None
+    if world == 1 and not args.skip_cpu:
+        threads = os.cpu_count() or 1
+        cwl = dict(kind="batch", field=field, width=128, log_blowup=lb, p2w=p2w, log_h=22)
+        log_rows = pick_cpu_sample(cwl, threads, budget_s=8.0)
+        dts = [cpu_commit_sample(dict(cwl, field=field), log_rows, threads) for _ in range(2)]
+        best = min(dts)
+        cpu = {"value": best[1] / best[0], "unit": "cells/s", "cores": threads, "kind": "port",
+               "sample": f"2^{log_rows} x 128 trace (the batch's mean width; LDE x2^{lb} + MMCS), best of 2, "
+                         "oracle/ C restatement"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_batch / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32" if field == 0 else "u64",
+        "data": "synthetic (seeded uniform field elements)",
+        "config": {"workload": args.workload, "n_traces": len(shapes), "log_rows": [wl["log_h_lo"], wl["log_h_hi"]],
+                   "widths": [wl["w_step"], wl["w_hi"]], "shape_seed": wl["seed"], "total_cells": cells,
+                   "log_blowup": lb, "poseidon2_width": p2w, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (%.1f GB of traces)" % (cells * esize / 1e9),
+                   "branches": info["branches"], "leaf_threads": info["leaf_threads"],
+                   "graph_kernels": info["kernels_per_run"], "plan_device_gb": info["device_bytes"] / 1e9,
+                   "plan_create_s": create_s, "tune_ms": info["tune_ms"]},
+        "plain": {"value": plain, "ms_per_step": 1e3 * t_plain / args.steps,
+                  "launches_per_step": plain_launches / args.steps,
+                  "path": "64 x zkb_pcs_commit_dev on the same device-resident traces"},
+        "batched_vs_plain": value / plain,
+        "e2e": {"value": cells * args.steps * world / t_e2e, "unit": "cells/s",
+                "h2d_bytes_per_step": cells * esize, "d2h_bytes_per_step": len(shapes) * digest * esize,
+                "ms_per_step": 1e3 * t_e2e / args.steps,
+                "path": "zkb_batch_copy_in (pinned) x64 + zkb_batch_run + zkb_batch_roots",
+                "plain_value": cells * args.steps * world / t_e2e_plain,
+                "plain_path": "64 x zkb_pcs_commit from pinned host memory"},
+        "roofline": {"kernel": "whole batched step (LDE + leaf hashing + compression)", "bound": "int",
+                     "unit": "Gmul/s", "achieved": ach, "peak": mul_peak / 1e9, "frac": ach / (mul_peak / 1e9),
+                     "peak_source": "measured in this run: zkb_measure_mul_peak",
+                     "work_per_step": f"{muls} Poseidon2 field mults", "traffic": None},
+        "cpu_baseline": cpu,
+        "gpu_launches": info["kernels_per_run"] * args.steps,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    batch.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -431,6 +638,8 @@ def main() -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, wl, rank, world)
+    if wl.get("kind") == "batch":
+        return run_batch(args, wl, rank, world, local_rank)
     return run_ours(args, wl, rank, world, local_rank)
 
 

@@ -147,6 +147,15 @@ ZKB_API int zkb_coset_lde_batch(int field, const void *trace, uint32_t log_h, ui
 ZKB_API int zkb_coset_lde_batch_dev(int field, const void *d_trace, uint32_t log_h, uint32_t width,
                             uint32_t log_blowup, uint64_t shift, int bitrev_rows, void *d_out,
                             void *stream);
+/* The device LDE (generator shift, bit-reversed rows) with explicit kernel shapes:
+ * largest NTT pass kmax index bits (1..11 BabyBear, 1..10 Goldilocks; 0 = default) and
+ * columns per CTA of the plain passes (1/4/8/16, 0 = default) and of the fused middle
+ * kernel (1/4/8, 0 = default).  Every choice gives the same output; the batched plan's
+ * autotuner picks among them.  No counterpart in the reference (its Metal NTT has one
+ * fixed dispatch shape, zkf-metal/src/ntt/p3_adapter.rs:78-294). */
+ZKB_API int zkb_coset_lde_tuned_dev(int field, const void *d_trace, uint32_t log_h, uint32_t width,
+                                    uint32_t log_blowup, int kmax, uint32_t c_pass, uint32_t c_fused,
+                                    void *d_out, void *stream);
 
 /* ------------------------------------------------------------------- MMCS */
 /* A row-major matrix: `data` is a host or device pointer depending on the call. */
@@ -321,6 +330,54 @@ ZKB_API int zkb_engine_wait(zkb_engine *engine, uint64_t job_id, zkb_job_result 
 ZKB_API int zkb_engine_stats(zkb_engine *engine, zkb_engine_stats_t *stats);
 /* Finishes the queued jobs, then stops the workers. */
 ZKB_API void zkb_engine_destroy(zkb_engine *engine);
+
+/* ------------------------------------------------------------------ batched commit
+ * Many traces of uneven height and width committed by one plan.  Replaces a loop of
+ * per-trace commits (TwoAdicFriPcs::commit over one matrix each,
+ * zkf-metal/src/merkle.rs:55-138 with the LDE of zkf-metal/src/ntt/p3_adapter.rs:78-294);
+ * every root equals that trace's plain commitment (zkb_pcs_commit).
+ * zkb_batch_create allocates every device buffer once, builds the tables, picks the
+ * kernel shapes (timed candidates when `autotune`, cached as JSON lines in
+ * `tune_cache`) and captures one CUDA graph; zkb_batch_run replays it.  A plan is
+ * used by one thread at a time; runs on different streams must not overlap. */
+typedef struct {
+  uint32_t log_h;        /* trace height 2^log_h */
+  uint32_t width;        /* columns, 1..4096 */
+} zkb_batch_shape;
+typedef struct {
+  uint32_t log_blowup;   /* 1..4 */
+  int use_graph;         /* 1: one CUDA graph per run; 0: the same launches on streams */
+  uint32_t branches;     /* concurrent LDE branches (1..8); 0 = tuned/default */
+  int autotune;          /* time kernel-shape candidates at creation */
+  const char *tune_cache;/* JSON-lines file read (and rewritten after tuning); NULL = none */
+} zkb_batch_options;
+typedef struct {
+  uint64_t device_bytes; /* the plan's arena */
+  uint32_t kernels_per_run; /* kernel nodes of the graph (0 without a graph) */
+  uint32_t branches;
+  uint32_t leaf_threads;
+  int use_graph;
+  int tuned_from_cache;
+  double tune_ms;        /* device time spent building tables and tuning */
+} zkb_batch_info_t;
+typedef struct zkb_batch zkb_batch;
+ZKB_API int zkb_batch_create(const zkb_hasher *hasher, const zkb_batch_shape *shapes, size_t n,
+                             const zkb_batch_options *options, zkb_batch **batch_out);
+/* Device buffer of trace i (2^log_h x width, row-major), for callers that write it in place. */
+ZKB_API int zkb_batch_trace_ptr(zkb_batch *batch, size_t i, void **d_trace);
+/* Copies trace i in from host (pinned for full bandwidth) or device memory. */
+ZKB_API int zkb_batch_copy_in(zkb_batch *batch, size_t i, const void *src, int src_on_device, void *stream);
+ZKB_API int zkb_batch_run(zkb_batch *batch, void *stream);
+/* n x OUT root elements (Goldilocks digests as u64); synchronises `stream`. */
+ZKB_API int zkb_batch_roots(zkb_batch *batch, void *roots_out, void *stream);
+/* Borrowed tree of trace i (valid while the plan lives, contents after a finished run):
+ * zkb_mmcs_open_batch and the zkb_tree_* accessors work on it; do not free it. */
+ZKB_API int zkb_batch_tree(zkb_batch *batch, size_t i, const zkb_tree **tree);
+ZKB_API int zkb_batch_info(const zkb_batch *batch, zkb_batch_info_t *info);
+/* Kernel shapes chosen for trace i's LDE (0 = default). */
+ZKB_API int zkb_batch_lde_tune(const zkb_batch *batch, size_t i, int *kmax, uint32_t *c_pass,
+                               uint32_t *c_fused);
+ZKB_API void zkb_batch_free(zkb_batch *batch);
 
 #ifdef __cplusplus
 }

@@ -7,6 +7,7 @@ This package is the host-side mirror of the reference's accelerator types.
 from ._native import ZkbDeclined, ZkbError, device_count, load  # noqa: F401
 from .accel import (  # noqa: F401
     BABYBEAR,
+    BatchCommit,
     CommitEngine,
     GOLDILOCKS,
     CudaDft,

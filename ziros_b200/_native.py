@@ -71,6 +71,21 @@ class JobResult(C.Structure):
                 ("run_ms", C.c_double), ("latency_ms", C.c_double)]
 
 
+class BatchShape(C.Structure):
+    _fields_ = [("log_h", C.c_uint32), ("width", C.c_uint32)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("log_blowup", C.c_uint32), ("use_graph", C.c_int), ("branches", C.c_uint32),
+                ("autotune", C.c_int), ("tune_cache", C.c_char_p)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("device_bytes", C.c_uint64), ("kernels_per_run", C.c_uint32), ("branches", C.c_uint32),
+                ("leaf_threads", C.c_uint32), ("use_graph", C.c_int), ("tuned_from_cache", C.c_int),
+                ("tune_ms", C.c_double)]
+
+
 class EngineStats(C.Structure):
     _fields_ = [("queued", C.c_uint64), ("completed", C.c_uint64), ("hbm_budget", C.c_uint64),
                 ("hbm_in_use", C.c_uint64), ("hbm_peak", C.c_uint64)]
@@ -130,6 +145,16 @@ SIGNATURES = {
     "zkb_engine_wait": (_I, [_P, _U64, _P, _P]),
     "zkb_engine_stats": (_I, [_P, _P]),
     "zkb_engine_destroy": (None, [_P]),
+    "zkb_coset_lde_tuned_dev": (_I, [_I, _P, _U32, _U32, _U32, _I, _U32, _U32, _P, _P]),
+    "zkb_batch_create": (_I, [_P, _P, _SZ, _P, _P]),
+    "zkb_batch_trace_ptr": (_I, [_P, _SZ, _P]),
+    "zkb_batch_copy_in": (_I, [_P, _SZ, _P, _I, _P]),
+    "zkb_batch_run": (_I, [_P, _P]),
+    "zkb_batch_roots": (_I, [_P, _P, _P]),
+    "zkb_batch_tree": (_I, [_P, _SZ, _P]),
+    "zkb_batch_info": (_I, [_P, _P]),
+    "zkb_batch_lde_tune": (_I, [_P, _SZ, _P, _P, _P]),
+    "zkb_batch_free": (None, [_P]),
     "zkb_pcs_commit_fri_dev": (_I, [_P, _P, _U32, _U32, _U32, _P, _P, _P, _P, _P, _P]),
 }
 

@@ -159,20 +159,33 @@ class CudaDft:
                                                  shift or 0, int(bit_reverse_rows), op, stream))
 
 
+    def coset_lde_tuned_dev(self, trace, log_blowup: int, out, kmax: int = 0, c_pass: int = 0,
+                            c_fused: int = 0) -> None:
+        """Device LDE (bit-reversed rows) with explicit kernel shapes (0 = default)."""
+        h, w = trace.shape
+        tp, stream = _torch_ptr_stream(trace)
+        op, _ = _torch_ptr_stream(out)
+        if out.shape[0] != h << log_blowup or out.shape[1] != w:
+            raise ValueError("output shape mismatch")
+        N.check(N.load().zkb_coset_lde_tuned_dev(self.field, tp, h.bit_length() - 1, w, log_blowup, kmax, c_pass,
+                                                 c_fused, op, stream))
+
+
 # -------------------------------------------------------------------------- MMCS
 class Tree:
     """Prover data of a commitment (p3 MerkleTree): digest layers stay on the device."""
 
-    def __init__(self, handle: C.c_void_p, field: int, shapes: Sequence[Tuple[int, int]]):
+    def __init__(self, handle: C.c_void_p, field: int, shapes: Sequence[Tuple[int, int]], owner=None):
         self._h = handle
         self.field = field
         self.heights = [int(s[0]) for s in shapes]
         self.widths = [int(s[1]) for s in shapes]
+        self._owner = owner  # a borrowed tree keeps the object that owns it alive
 
     def __del__(self):
         h = getattr(self, "_h", None)
         self._h = None
-        if h:
+        if h and getattr(self, "_owner", None) is None:
             try:
                 N.load().zkb_tree_free(h)
             except Exception:  # interpreter shutdown: module state already torn down
@@ -518,3 +531,91 @@ class CommitEngine:
 
     def __del__(self):
         self.close()
+
+
+# ------------------------------------------------------------------ batched commit
+class BatchCommit:
+    """Many traces of uneven height and width committed by one plan (zkb_batch_*): one
+    device arena, tables built once, kernel shapes autotuned (JSON-lines cache), and one
+    CUDA graph per run.  Every root equals the trace's plain commitment
+    (CudaTwoAdicPcs.commit)."""
+
+    def __init__(self, shapes: Sequence[Tuple[int, int]], field: int = BABYBEAR, seed: int = 42,
+                 log_blowup: int = 1, p2_width: int = 16, use_graph: bool = True, branches: int = 0,
+                 autotune: bool = True, tune_cache: Optional[str] = None):
+        lib = N.load()
+        self.field = field
+        self.shapes = [(int(h), int(w)) for h, w in shapes]
+        for h, w in self.shapes:
+            if h <= 0 or h & (h - 1):
+                raise ValueError("trace heights must be powers of two")
+        self.log_blowup = log_blowup
+        self.digest_elems = 8 if p2_width == 16 else 4
+        self.hasher = N.Hasher(field, p2_width, seed)
+        arr = (N.BatchShape * len(self.shapes))(*[N.BatchShape(h.bit_length() - 1, w) for h, w in self.shapes])
+        opt = N.BatchOptions(log_blowup, int(use_graph), branches, int(autotune),
+                             tune_cache.encode() if tune_cache else None)
+        self._h = C.c_void_p()
+        N.check(lib.zkb_batch_create(C.byref(self.hasher), arr, len(self.shapes), C.byref(opt), C.byref(self._h)))
+
+    def __len__(self):
+        return len(self.shapes)
+
+    def copy_in(self, i: int, trace, stream=None) -> None:
+        """trace: a host array, a pinned host torch tensor (asynchronous: keep it alive
+        until the stream has passed the copy) or a CUDA torch tensor."""
+        lib = N.load()
+        h, w = self.shapes[i]
+        if hasattr(trace, "is_cuda"):
+            if tuple(trace.shape) != (h, w) or trace.element_size() != np.dtype(dtype_of(self.field)).itemsize:
+                raise ValueError("trace shape/type mismatch")
+            s = stream if stream is not None else _current_stream(trace)
+            N.check(lib.zkb_batch_copy_in(self._h, i, C.c_void_p(trace.data_ptr()), int(trace.is_cuda), s))
+            return
+        a = np.ascontiguousarray(trace, dtype=dtype_of(self.field))
+        if a.shape != (h, w):
+            raise ValueError("trace shape mismatch")
+        # a pageable source is staged before the call returns
+        N.check(lib.zkb_batch_copy_in(self._h, i, _ptr(a), 0, stream))
+
+    def run(self, stream=None) -> None:
+        N.check(N.load().zkb_batch_run(self._h, stream))
+
+    def roots(self, stream=None) -> np.ndarray:
+        out = np.zeros((len(self), self.digest_elems), dtype=dtype_of(self.field))
+        N.check(N.load().zkb_batch_roots(self._h, _ptr(out), stream))
+        return out
+
+    def tree(self, i: int) -> Tree:
+        t = C.c_void_p()
+        N.check(N.load().zkb_batch_tree(self._h, i, C.byref(t)))
+        h, w = self.shapes[i]
+        return Tree(t, self.field, [(h << self.log_blowup, w)], owner=self)
+
+    def info(self) -> dict:
+        st = N.BatchInfo()
+        N.check(N.load().zkb_batch_info(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in N.BatchInfo._fields_}
+
+    def lde_tune(self, i: int) -> Tuple[int, int, int]:
+        k, cp, cf = C.c_int(), C.c_uint32(), C.c_uint32()
+        N.check(N.load().zkb_batch_lde_tune(self._h, i, C.byref(k), C.byref(cp), C.byref(cf)))
+        return k.value, cp.value, cf.value
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h:
+            try:
+                N.load().zkb_batch_free(h)
+            except Exception:  # interpreter shutdown
+                pass
+
+    def __del__(self):
+        self.close()
+
+
+def _current_stream(t):
+    import torch
+
+    return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)

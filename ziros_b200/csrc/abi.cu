@@ -229,6 +229,24 @@ int zkb_dft_batch(int field, void *rowmajor, uint32_t log_h, uint32_t width, int
   return to_host(rowmajor, d.p, bytes, s);
 }
 
+int zkb_coset_lde_tuned_dev(int field, const void *d_trace, uint32_t log_h, uint32_t width,
+                            uint32_t log_blowup, int kmax, uint32_t c_pass, uint32_t c_fused,
+                            void *d_out, void *stream) {
+  ZKB_ENTRY();
+  ZKB_TRY(check_field(field));
+  LdeTune t;
+  t.kmax = kmax;
+  t.c_pass = c_pass;
+  t.c_fused = c_fused;
+  ZKB_TRY(lde_tune_check(field, width, t));
+  cudaStream_t s = resolve_stream(stream);
+  if (field == ZKB_FIELD_BABYBEAR)
+    return ntt_lde_dev<BabyBear>((const uint32_t *)d_trace, (int)log_h, width, (int)log_blowup,
+                                 BabyBear::GENERATOR, true, (uint32_t *)d_out, s, &t);
+  return ntt_lde_dev<Goldilocks>((const uint64_t *)d_trace, (int)log_h, width, (int)log_blowup,
+                                 Goldilocks::GENERATOR, true, (uint64_t *)d_out, s, &t);
+}
+
 int zkb_coset_lde_batch_dev(int field, const void *d_trace, uint32_t log_h, uint32_t width,
                             uint32_t log_blowup, uint64_t shift, int bitrev_rows, void *d_out,
                             void *stream) {

@@ -1,0 +1,849 @@
+// batch.cu — batched commitment of many traces of uneven height and width.
+//
+// A plan (zkb_batch_create) owns one device arena with every trace's input, LDE and
+// digest layers, builds the twiddle and coset tables, and chooses kernel shapes
+// (autotuned and cached, or defaults).  A run is one CUDA graph:
+//
+//   fork -> per branch, the coset LDEs of its traces (ntt passes + fused middle kernel,
+//           coefficient scratch owned by the branch)
+//   join -> ONE leaf-hash launch over the rows of all traces (job table, binary search
+//           of the trace by row)
+//        -> one compression launch per tree level, across every tree that still has
+//           that level
+//        -> one launch gathering the roots
+//
+// Every trace gets exactly the p3 MerkleTree of its own LDE (power-of-two heights: no
+// padding, no injection), so each root equals the plain per-trace commitment
+// (TwoAdicFriPcs::commit over one matrix, vendor/p3-merkle-tree-gpu/src/merkle_tree.rs:84-151).
+// The reference commits each trace with its own dispatch sequence; the plan is this
+// library's batched form of that call.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <numeric>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "poseidon2.cuh"
+
+namespace zkb {
+namespace {
+
+constexpr int MAX_BATCH = 1024;
+
+struct LeafJob {
+  const void *lde;     // N x width, row-major, bit-reversed rows
+  void *digests;       // N x OUT
+  uint64_t row_start;  // prefix over the jobs
+  uint64_t rows;
+  uint64_t width;
+};
+
+struct CompJob {
+  const void *prev;  // 2 * n_out digests
+  void *next;        // n_out digests
+  uint64_t start;    // prefix over the jobs of one level
+  uint64_t n_out;
+};
+
+template <int W>
+constexpr int digest_len() {
+  return W == 16 ? 8 : 4;
+}
+
+// index of the last job whose start <= g (starts ascending, starts[0] = 0)
+__device__ __forceinline__ int find_job(const uint64_t *starts, int n, uint64_t g) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (starts[mid] <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// PaddingFreeSponge leaf digest of every row of every job (one permutation call site).
+template <class F, int W>
+__global__ void __launch_bounds__(256)
+    batch_leaf_kernel(const LeafJob *__restrict__ jobs, int n_jobs, uint64_t total_rows,
+                      const __grid_constant__ P2Params<F, W> p) {
+  using T = typename F::T;
+  using D = Dom<F>;
+  constexpr int OUT = digest_len<W>();
+  extern __shared__ uint64_t starts[];  // n_jobs entries
+  for (int i = threadIdx.x; i < n_jobs; i += blockDim.x) starts[i] = jobs[i].row_start;
+  __syncthreads();
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total_rows;
+       g += (uint64_t)gridDim.x * blockDim.x) {
+    const int j = find_job(starts, n_jobs, g);
+    const uint64_t row = g - starts[j];
+    const uint64_t width = jobs[j].width;
+    const T *rp = (const T *)jobs[j].lde + row * width;
+    T s[W];
+#pragma unroll
+    for (int i = 0; i < W; i++) s[i] = 0;
+    for (uint64_t c = 0; c < width; c += 8) {
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if (c + i < width) s[i] = D::enter(rp[c + i]);
+      p2_permute<F, W>(s, p);
+    }
+    T *out = (T *)jobs[j].digests + row * OUT;
+#pragma unroll
+    for (int i = 0; i < OUT; i++) out[i] = D::leave(s[i]);
+  }
+}
+
+// next[i] = compress(prev[2i], prev[2i+1]) for every job of one tree level.
+template <class F, int W>
+__global__ void __launch_bounds__(128)
+    batch_compress_kernel(const CompJob *__restrict__ jobs, int n_jobs, uint64_t total,
+                          const __grid_constant__ P2Params<F, W> p) {
+  using T = typename F::T;
+  using D = Dom<F>;
+  constexpr int OUT = digest_len<W>();
+  extern __shared__ uint64_t starts[];  // n_jobs entries
+  for (int i = threadIdx.x; i < n_jobs; i += blockDim.x) starts[i] = jobs[i].start;
+  __syncthreads();
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (uint64_t)gridDim.x * blockDim.x) {
+    const int j = find_job(starts, n_jobs, g);
+    const uint64_t i = g - starts[j];
+    const T *prev = (const T *)jobs[j].prev;
+    T s[W];
+#pragma unroll
+    for (int k = 0; k < OUT; k++) {
+      s[k] = D::enter(prev[(2 * i) * OUT + k]);
+      s[OUT + k] = D::enter(prev[(2 * i + 1) * OUT + k]);
+    }
+#pragma unroll
+    for (int k = 2 * OUT; k < W; k++) s[k] = 0;
+    p2_permute<F, W>(s, p);
+    T *next = (T *)jobs[j].next + i * OUT;
+#pragma unroll
+    for (int k = 0; k < OUT; k++) next[k] = D::leave(s[k]);
+  }
+}
+
+template <class T, int OUT>
+__global__ void batch_roots_kernel(const uint64_t *__restrict__ root_off, const T *__restrict__ digests,
+                                   int n, T *__restrict__ roots) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n * OUT) roots[t] = digests[root_off[t / OUT] * OUT + (t % OUT)];
+}
+
+uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
+
+uint64_t fnv1a(const void *data, size_t n, uint64_t h = 1469598103934665603ull) {
+  const unsigned char *p = (const unsigned char *)data;
+  for (size_t i = 0; i < n; i++) h = (h ^ p[i]) * 1099511628211ull;
+  return h;
+}
+
+// ---- tuning cache: one JSON object per line, {"key": "...", "name": int, ...}
+struct TuneCache {
+  std::string path;
+  std::vector<std::pair<std::string, std::string>> lines;  // key, full line
+
+  void load() {
+    if (path.empty()) return;
+    std::ifstream f(path);
+    std::string ln;
+    while (std::getline(f, ln)) {
+      const size_t k = ln.find("\"key\": \"");
+      if (k == std::string::npos) continue;
+      const size_t a = k + 8, b = ln.find('"', a);
+      if (b == std::string::npos) continue;
+      lines.emplace_back(ln.substr(a, b - a), ln);
+    }
+  }
+  const std::string *find(const std::string &key) const {
+    for (auto &kv : lines)
+      if (kv.first == key) return &kv.second;
+    return nullptr;
+  }
+  static bool field(const std::string &line, const char *name, long *out) {
+    const std::string pat = std::string("\"") + name + "\": ";
+    const size_t k = line.find(pat);
+    if (k == std::string::npos) return false;
+    *out = strtol(line.c_str() + k + pat.size(), nullptr, 10);
+    return true;
+  }
+  void put(const std::string &key, const std::string &line) {
+    for (auto &kv : lines)
+      if (kv.first == key) {
+        kv.second = line;
+        return;
+      }
+    lines.emplace_back(key, line);
+  }
+  void save() const {
+    if (path.empty()) return;
+    const std::string tmp = path + ".tmp";
+    {
+      std::ofstream f(tmp, std::ios::trunc);
+      if (!f) return;
+      for (auto &kv : lines) f << kv.second << "\n";
+    }
+    std::rename(tmp.c_str(), path.c_str());
+  }
+};
+
+}  // namespace
+}  // namespace zkb
+
+using namespace zkb;
+
+struct zkb_batch {
+  int device = 0;
+  HasherSpec spec;
+  uint32_t log_b = 1;
+  size_t es = 4;
+  int out = 8;
+  std::vector<zkb_batch_shape> shapes;
+  // arena
+  void *arena = nullptr;
+  uint64_t arena_bytes = 0;
+  std::vector<void *> d_in, d_lde, d_layers;
+  std::vector<std::vector<uint64_t>> layer_len;  // per trace, in digests
+  std::vector<void *> d_coef;                    // per branch: scratch for its largest trace
+  uint64_t coef_bytes = 0;
+  void *d_roots = nullptr;
+  uint64_t *d_root_off = nullptr;  // digest offsets of the roots from d_layers[0]
+  LeafJob *d_leaf_jobs = nullptr;
+  CompJob *d_comp_jobs = nullptr;
+  uint64_t total_rows = 0;
+  std::vector<size_t> lvl_off, lvl_cnt;
+  std::vector<uint64_t> lvl_total;
+  // kernel shapes
+  std::vector<LdeTune> tune;  // per trace
+  unsigned leaf_threads = 128;
+  uint32_t branches = 1;
+  std::vector<std::vector<int>> branch_traces;
+  bool use_graph = true;
+  bool tuned_from_cache = false;
+  double tune_ms = 0;
+  // execution
+  cudaStream_t s_main = nullptr;
+  std::vector<cudaStream_t> s_br;
+  std::vector<cudaEvent_t> ev_br;
+  cudaEvent_t ev_fork = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint32_t kernels_per_run = 0;
+  P2Params<BabyBear, 16> p_bb16;
+  P2Params<Goldilocks, 16> p_gl16;
+  P2Params<Goldilocks, 12> p_gl12;
+  std::vector<std::unique_ptr<zkb_tree>> trees;
+
+  ~zkb_batch() {
+    cudaSetDevice(device);
+    if (s_main) cudaStreamSynchronize(s_main);
+    trees.clear();
+    if (!d_coef.empty()) cudaFree(d_coef[0]);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (auto e : ev_br) cudaEventDestroy(e);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    for (auto s : s_br) cudaStreamDestroy(s);
+    if (s_main) cudaStreamDestroy(s_main);
+    if (arena) cudaFree(arena);
+  }
+
+  uint64_t rows_of(size_t i) const { return 1ull << (shapes[i].log_h + log_b); }
+
+  // ---- launches of one run, enqueued on `origin` (captured or direct)
+  int lde_one(size_t i, cudaStream_t s, const LdeTune *t) {
+    const int lh = (int)shapes[i].log_h;
+    const uint32_t w = shapes[i].width;
+    const int br = branch_of(i);
+    if (spec.field == FIELD_BABYBEAR)
+      return ntt_lde_dev<BabyBear>((const uint32_t *)d_in[i], lh, w, (int)log_b, BabyBear::GENERATOR, true,
+                                   (uint32_t *)d_lde[i], s, t, (uint32_t *)d_coef[br]);
+    return ntt_lde_dev<Goldilocks>((const uint64_t *)d_in[i], lh, w, (int)log_b, Goldilocks::GENERATOR, true,
+                                   (uint64_t *)d_lde[i], s, t, (uint64_t *)d_coef[br]);
+  }
+  int branch_of(size_t i) const {
+    for (size_t b = 0; b < branch_traces.size(); b++)
+      for (int t : branch_traces[b])
+        if ((size_t)t == i) return (int)b;
+    return 0;
+  }
+
+  template <class F, int W>
+  int hash_all(const P2Params<F, W> &p, unsigned threads, cudaStream_t s) {
+    DeviceContext *ctx;
+    ZKB_TRY(current_context(&ctx));
+    const int n = (int)shapes.size();
+    ZKB_LAUNCH("batch_leaf_hash", s, batch_leaf_kernel<F, W><<<grid_for(total_rows, threads, (unsigned)ctx->sm_count * (2048u / threads)), threads, n * sizeof(uint64_t), s>>>(d_leaf_jobs, n, total_rows, p));
+    for (size_t l = 0; l < lvl_cnt.size(); l++) {
+      ZKB_LAUNCH("batch_compress", s, batch_compress_kernel<F, W><<<grid_for(lvl_total[l], 128, (unsigned)ctx->sm_count * 16u), 128, lvl_cnt[l] * sizeof(uint64_t), s>>>(d_comp_jobs + lvl_off[l], (int)lvl_cnt[l], lvl_total[l], p));
+    }
+    using T = typename F::T;
+    constexpr int OUT = digest_len<W>();
+    ZKB_LAUNCH("batch_roots", s, batch_roots_kernel<T, OUT><<<(n * OUT + 127) / 128, 128, 0, s>>>(d_root_off, (const T *)d_layers[0], n, (T *)d_roots));
+    return ZKB_OK;
+  }
+
+  int hash_dispatch(unsigned threads, cudaStream_t s) {
+    if (spec.field == FIELD_BABYBEAR) return hash_all<BabyBear, 16>(p_bb16, threads, s);
+    if (spec.width == 16) return hash_all<Goldilocks, 16>(p_gl16, threads, s);
+    return hash_all<Goldilocks, 12>(p_gl12, threads, s);
+  }
+
+  int enqueue(cudaStream_t origin) {
+    const uint32_t nb = (uint32_t)branch_traces.size();
+    ZKB_CHECK_CUDA(cudaEventRecord(ev_fork, origin));
+    for (uint32_t b = 0; b < nb; b++) {
+      ZKB_CHECK_CUDA(cudaStreamWaitEvent(s_br[b], ev_fork, 0));
+      for (int i : branch_traces[b]) ZKB_TRY(lde_one((size_t)i, s_br[b], &tune[i]));
+      ZKB_CHECK_CUDA(cudaEventRecord(ev_br[b], s_br[b]));
+      ZKB_CHECK_CUDA(cudaStreamWaitEvent(origin, ev_br[b], 0));
+    }
+    return hash_dispatch(leaf_threads, origin);
+  }
+
+  // Longest-processing-time assignment of the traces to `nb` branches; each branch gets
+  // coefficient scratch for its largest trace.  Fails (without changing the current
+  // assignment) when that scratch does not fit in free device memory.
+  int assign_branches(uint32_t nb) {
+    std::vector<std::vector<int>> bt(nb);
+    std::vector<int> ord(shapes.size());
+    std::iota(ord.begin(), ord.end(), 0);
+    auto cost = [&](int i) { return (double)rows_of(i) * shapes[i].width * (shapes[i].log_h + log_b + 1); };
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    std::vector<double> load(nb, 0.0);
+    for (int i : ord) {
+      const size_t b = std::min_element(load.begin(), load.end()) - load.begin();
+      bt[b].push_back(i);
+      load[b] += cost(i);
+    }
+    std::vector<uint64_t> need(nb, 0);
+    uint64_t total = 0;
+    for (uint32_t b = 0; b < nb; b++) {
+      for (int i : bt[b]) need[b] = std::max<uint64_t>(need[b], (1ull << shapes[i].log_h) * shapes[i].width * es);
+      need[b] = align256(std::max<uint64_t>(need[b], 256));
+      total += need[b];
+    }
+    size_t free_b = 0, total_b = 0;
+    ZKB_CHECK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const uint64_t avail = free_b + coef_bytes;  // the current scratch is released first
+    ZKB_REQUIRE(total + (1ull << 30) <= avail, "%u branches need %llu bytes of scratch, %llu available", nb,
+                (unsigned long long)total, (unsigned long long)avail);
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    ZKB_CHECK_CUDA(cudaStreamSynchronize(s_main));
+    if (!d_coef.empty()) cudaFree(d_coef[0]);
+    d_coef.clear();
+    coef_bytes = 0;
+    void *scratch = nullptr;
+    ZKB_CHECK_CUDA(cudaMalloc(&scratch, total));
+    d_coef.push_back(scratch);
+    for (uint32_t b = 1; b < nb; b++) d_coef.push_back((char *)d_coef[b - 1] + need[b - 1]);
+    coef_bytes = total;
+    branch_traces = std::move(bt);
+    branches = nb;
+    return ZKB_OK;
+  }
+
+  int capture() {
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    if (graph) {
+      cudaGraphDestroy(graph);
+      graph = nullptr;
+    }
+    ZKB_CHECK_CUDA(cudaStreamBeginCapture(s_main, cudaStreamCaptureModeRelaxed));
+    const int rc = enqueue(s_main);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s_main, &g);
+    ZKB_TRY(rc);
+    if (e != cudaSuccess) {
+      set_error("graph capture failed: %s", cudaGetErrorString(e));
+      return ZKB_ERR_CUDA;
+    }
+    graph = g;
+    ZKB_CHECK_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    size_t nn = 0;
+    ZKB_CHECK_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    ZKB_CHECK_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
+    kernels_per_run = 0;
+    for (auto nd : nodes) {
+      cudaGraphNodeType ty;
+      ZKB_CHECK_CUDA(cudaGraphNodeGetType(nd, &ty));
+      if (ty == cudaGraphNodeTypeKernel) kernels_per_run++;
+    }
+    return ZKB_OK;
+  }
+
+  int run(cudaStream_t s) {
+    if (use_graph) {
+      if (!exec) ZKB_TRY(capture());
+      ZKB_CHECK_CUDA(cudaGraphLaunch(exec, s));
+      return ZKB_OK;
+    }
+    return enqueue(s);
+  }
+
+  // ---- autotuning
+  // Times fn() on s_main with CUDA events: the best of `reps` after one warm-up.
+  template <class Fn>
+  int time_ms(Fn fn, int reps, float *best) {
+    cudaEvent_t a, b;
+    ZKB_CHECK_CUDA(cudaEventCreate(&a));
+    ZKB_CHECK_CUDA(cudaEventCreate(&b));
+    *best = 1e30f;
+    int rc = ZKB_OK;
+    for (int r = 0; r <= reps && rc == ZKB_OK; r++) {
+      cudaEventRecord(a, s_main);
+      rc = fn();
+      cudaEventRecord(b, s_main);
+      if (rc == ZKB_OK && cudaEventSynchronize(b) != cudaSuccess) rc = ZKB_ERR_CUDA;
+      float ms = 0;
+      if (rc == ZKB_OK && r > 0 && cudaEventElapsedTime(&ms, a, b) == cudaSuccess) *best = std::min(*best, ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc == ZKB_ERR_CUDA) set_error("timing run failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return rc;
+  }
+
+  std::string lde_key(size_t i) const {
+    char k[96];
+    snprintf(k, sizeof k, "lde/%d/%u/%u/%u", spec.field, shapes[i].log_h, shapes[i].width, log_b);
+    return k;
+  }
+
+  int tune_lde(TuneCache &cache, bool autotune) {
+    const int kdef = spec.field == FIELD_BABYBEAR ? 11 : 10;
+    std::vector<std::pair<std::string, LdeTune>> done;
+    for (size_t i = 0; i < shapes.size(); i++) {
+      const std::string key = lde_key(i);
+      bool found = false;
+      for (auto &d : done)
+        if (d.first == key) {
+          tune[i] = d.second;
+          found = true;
+        }
+      if (found) continue;
+      if (const std::string *ln = cache.find(key)) {
+        long km = 0, cp = 0, cf = 0;
+        LdeTune t;
+        if (TuneCache::field(*ln, "kmax", &km) && TuneCache::field(*ln, "c_pass", &cp) &&
+            TuneCache::field(*ln, "c_fused", &cf)) {
+          t.kmax = (int)km;
+          t.c_pass = (uint32_t)cp;
+          t.c_fused = (uint32_t)cf;
+          if (lde_tune_check(spec.field, shapes[i].width, t) == ZKB_OK) {
+            tune[i] = t;
+            done.emplace_back(key, t);
+            tuned_from_cache = true;
+            continue;
+          }
+          clear_error();
+        }
+      }
+      if (!autotune) {
+        tune[i] = LdeTune{};
+        continue;
+      }
+      const uint32_t w = shapes[i].width;
+      std::vector<LdeTune> cands;
+      std::vector<std::vector<int>> seen_plans;
+      for (int km = kdef; km >= kdef - 2 && km >= 1; km--) {
+        // kernel choices only differ when the pass split does
+        std::vector<int> ks;
+        const int L = (int)shapes[i].log_h;
+        const int np = L > 0 ? (L + km - 1) / km : 0;
+        for (int q = 0; q < np; q++) ks.push_back(L / np + (q < L % np ? 1 : 0));
+        if (std::find(seen_plans.begin(), seen_plans.end(), ks) != seen_plans.end()) continue;
+        seen_plans.push_back(ks);
+        for (uint32_t cp : {16u, 8u, 4u})
+          for (uint32_t cf : {8u, 4u}) {
+            LdeTune t{km, cp, cf};
+            if (lde_tune_check(spec.field, w, t) != ZKB_OK) {
+              clear_error();
+              continue;
+            }
+            cands.push_back(t);
+          }
+      }
+      if (cands.empty()) cands.push_back(LdeTune{});
+      LdeTune best_t = cands[0];
+      float best = 1e30f;
+      for (const LdeTune &t : cands) {
+        float ms = 0;
+        ZKB_TRY(time_ms([&] { return lde_one(i, s_main, &t); }, 2, &ms));
+        if (ms < best) {
+          best = ms;
+          best_t = t;
+        }
+      }
+      tune[i] = best_t;
+      done.emplace_back(key, best_t);
+      char ln[256];
+      snprintf(ln, sizeof ln, "{\"key\": \"%s\", \"kmax\": %d, \"c_pass\": %u, \"c_fused\": %u, \"us\": %d}",
+               key.c_str(), best_t.kmax, best_t.c_pass, best_t.c_fused, (int)(best * 1000));
+      cache.put(key, ln);
+    }
+    return ZKB_OK;
+  }
+
+  std::string batch_key(const char *what) const {
+    std::vector<uint32_t> sig;
+    for (auto &s : shapes) {
+      sig.push_back(s.log_h);
+      sig.push_back(s.width);
+    }
+    const uint64_t h = fnv1a(sig.data(), sig.size() * 4);
+    char k[128];
+    snprintf(k, sizeof k, "%s/%d/%d/%u/%zu/%016llx", what, spec.field, spec.width, log_b, shapes.size(),
+             (unsigned long long)h);
+    return k;
+  }
+
+  int tune_leaf_and_branches(TuneCache &cache, bool autotune, uint32_t fixed_branches) {
+    const std::string lk = batch_key("leaf"), bk = batch_key("branches");
+    long v = 0;
+    if (const std::string *ln = cache.find(lk); ln && TuneCache::field(*ln, "threads", &v) &&
+                                                (v == 64 || v == 128 || v == 256)) {
+      leaf_threads = (unsigned)v;
+      tuned_from_cache = true;
+    } else if (autotune) {
+      float best = 1e30f;
+      for (unsigned th : {64u, 128u, 256u}) {
+        float ms = 0;
+        ZKB_TRY(time_ms([&] { return hash_dispatch(th, s_main); }, 2, &ms));
+        if (ms < best) {
+          best = ms;
+          leaf_threads = th;
+        }
+      }
+      char ln[256];
+      snprintf(ln, sizeof ln, "{\"key\": \"%s\", \"threads\": %u, \"us\": %d}", lk.c_str(), leaf_threads,
+               (int)(best * 1000));
+      cache.put(lk, ln);
+    }
+    if (fixed_branches) return assign_branches(fixed_branches);
+    if (const std::string *ln = cache.find(bk); ln && TuneCache::field(*ln, "branches", &v) && v >= 1 &&
+                                                v <= (long)s_br.size()) {
+      ZKB_TRY(assign_branches((uint32_t)v));
+      tuned_from_cache = true;
+      return ZKB_OK;
+    }
+    if (!autotune) {
+      // default: as many branches as fit, up to four
+      for (uint32_t nb = std::min<uint32_t>(4, (uint32_t)s_br.size()); nb >= 1; nb--) {
+        if (assign_branches(nb) == ZKB_OK) return ZKB_OK;
+        clear_error();
+      }
+      return assign_branches(1);
+    }
+    float best = 1e30f;
+    uint32_t best_nb = 1;
+    for (uint32_t nb : {1u, 2u, 4u, 8u}) {
+      if (nb > shapes.size() || nb > s_br.size()) continue;
+      if (assign_branches(nb) != ZKB_OK) {  // scratch does not fit: fewer branches only
+        clear_error();
+        continue;
+      }
+      if (use_graph) ZKB_TRY(capture());
+      float ms = 0;
+      ZKB_TRY(time_ms([&] { return run(s_main); }, 2, &ms));
+      if (ms < best) {
+        best = ms;
+        best_nb = nb;
+      }
+    }
+    ZKB_TRY(assign_branches(best_nb));
+    char ln[256];
+    snprintf(ln, sizeof ln, "{\"key\": \"%s\", \"branches\": %u, \"us\": %d}", bk.c_str(), best_nb,
+             (int)(best * 1000));
+    cache.put(bk, ln);
+    return ZKB_OK;
+  }
+};
+
+namespace {
+
+constexpr uint32_t MAX_BRANCHES = 8;
+
+int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
+  const size_t n = b->shapes.size();
+  const int OUT = b->out;
+  const size_t es = b->es;
+  const uint32_t nb_max = std::min<uint32_t>(MAX_BRANCHES, (uint32_t)n);
+  // ---- arena layout
+  uint64_t off = 0;
+  std::vector<uint64_t> in_off(n), lde_off(n), lay_off(n);
+  uint64_t total_digests = 0;
+  for (size_t i = 0; i < n; i++) {
+    const uint64_t rows = 1ull << b->shapes[i].log_h, w = b->shapes[i].width;
+    in_off[i] = off;
+    off = align256(off + rows * w * es);
+    lde_off[i] = off;
+    off = align256(off + (rows << b->log_b) * w * es);
+  }
+  const uint64_t layers_base = off;
+  for (size_t i = 0; i < n; i++) {
+    lay_off[i] = total_digests;  // digests from layers_base
+    total_digests += 2 * b->rows_of(i) - 1;
+  }
+  off = align256(off + total_digests * OUT * es);
+  const uint64_t roots_off = off;
+  off = align256(off + n * OUT * es);
+  const uint64_t root_off_off = off;
+  off = align256(off + n * 8);
+  const uint64_t leaf_jobs_off = off;
+  off = align256(off + n * sizeof(LeafJob));
+  // compression levels: level l exists for trace i when N_i > 2^l
+  int max_levels = 0;
+  for (size_t i = 0; i < n; i++) max_levels = std::max<int>(max_levels, (int)(b->shapes[i].log_h + b->log_b));
+  const uint64_t comp_jobs_off = off;
+  off = align256(off + (uint64_t)max_levels * n * sizeof(CompJob));
+  b->arena_bytes = off;
+
+  size_t free_b = 0, total_b = 0;
+  ZKB_CHECK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  ZKB_REQUIRE(b->arena_bytes + (1ull << 30) <= free_b,
+              "batch needs %llu bytes of device memory, %llu free", (unsigned long long)b->arena_bytes,
+              (unsigned long long)free_b);
+  ZKB_CHECK_CUDA(cudaMalloc(&b->arena, b->arena_bytes));
+  char *base = (char *)b->arena;
+  b->d_in.resize(n);
+  b->d_lde.resize(n);
+  b->d_layers.resize(n);
+  for (size_t i = 0; i < n; i++) {
+    b->d_in[i] = base + in_off[i];
+    b->d_lde[i] = base + lde_off[i];
+    b->d_layers[i] = base + layers_base + lay_off[i] * OUT * es;
+  }
+  b->d_roots = base + roots_off;
+  b->d_root_off = (uint64_t *)(base + root_off_off);
+  b->d_leaf_jobs = (LeafJob *)(base + leaf_jobs_off);
+  b->d_comp_jobs = (CompJob *)(base + comp_jobs_off);
+
+  // ---- job tables
+  std::vector<LeafJob> leaf(n);
+  std::vector<uint64_t> root_off(n);
+  uint64_t rs = 0;
+  b->layer_len.assign(n, {});
+  for (size_t i = 0; i < n; i++) {
+    const uint64_t N = b->rows_of(i);
+    leaf[i] = LeafJob{b->d_lde[i], b->d_layers[i], rs, N, b->shapes[i].width};
+    rs += N;
+    uint64_t o = 0;
+    for (uint64_t len = N;; len /= 2) {
+      b->layer_len[i].push_back(len);
+      if (len == 1) break;
+      o += len;
+    }
+    root_off[i] = lay_off[i] + o;
+  }
+  b->total_rows = rs;
+  std::vector<CompJob> comp;
+  for (int l = 0; l < max_levels; l++) {
+    b->lvl_off.push_back(comp.size());
+    uint64_t start = 0;
+    for (size_t i = 0; i < n; i++) {
+      const auto &ll = b->layer_len[i];
+      if ((size_t)l + 1 >= ll.size()) continue;
+      uint64_t lo = 0;
+      for (int q = 0; q < l; q++) lo += ll[q];
+      const char *lay = (const char *)b->d_layers[i];
+      comp.push_back(CompJob{lay + lo * OUT * es, (void *)(lay + (lo + ll[l]) * OUT * es), start, ll[l] / 2});
+      start += ll[l] / 2;
+    }
+    b->lvl_cnt.push_back(comp.size() - b->lvl_off.back());
+    b->lvl_total.push_back(start);
+  }
+  ZKB_CHECK_CUDA(cudaMemsetAsync(b->arena, 0, layers_base, b->s_main));
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(b->d_leaf_jobs, leaf.data(), n * sizeof(LeafJob), cudaMemcpyHostToDevice, b->s_main));
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(b->d_comp_jobs, comp.data(), comp.size() * sizeof(CompJob), cudaMemcpyHostToDevice,
+                                 b->s_main));
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(b->d_root_off, root_off.data(), n * 8, cudaMemcpyHostToDevice, b->s_main));
+  ZKB_CHECK_CUDA(cudaStreamSynchronize(b->s_main));
+
+  // ---- streams and events
+  for (uint32_t k = 0; k < nb_max; k++) {
+    cudaStream_t s;
+    ZKB_CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    b->s_br.push_back(s);
+    cudaEvent_t e;
+    ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->ev_br.push_back(e);
+  }
+  ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+
+  // ---- tables (built once, outside any capture) and kernel shapes
+  b->tune.assign(n, LdeTune{});
+  ZKB_TRY(b->assign_branches(1));
+  for (size_t i = 0; i < n; i++) ZKB_TRY(b->lde_one(i, b->s_main, nullptr));
+  ZKB_CHECK_CUDA(cudaStreamSynchronize(b->s_main));
+  TuneCache cache;
+  if (opt.tune_cache) cache.path = opt.tune_cache;
+  cache.load();
+  cudaEvent_t t0, t1;
+  ZKB_CHECK_CUDA(cudaEventCreate(&t0));
+  ZKB_CHECK_CUDA(cudaEventCreate(&t1));
+  cudaEventRecord(t0, b->s_main);
+  int rc = b->tune_lde(cache, opt.autotune != 0);
+  if (rc == ZKB_OK) rc = b->tune_leaf_and_branches(cache, opt.autotune != 0, std::min(opt.branches, nb_max));
+  cudaEventRecord(t1, b->s_main);
+  cudaEventSynchronize(t1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  b->tune_ms = ms;
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  ZKB_TRY(rc);
+  if (opt.autotune) cache.save();
+  if (b->use_graph) ZKB_TRY(b->capture());
+
+  // ---- borrowed per-trace trees for openings
+  for (size_t i = 0; i < n; i++) {
+    auto t = std::make_unique<zkb_tree>();
+    DeviceTree &d = t->t;
+    d.spec = b->spec;
+    d.device = b->device;
+    d.stream = b->s_main;
+    d.d_layers = b->d_layers[i];
+    d.borrowed = true;
+    uint64_t o = 0;
+    for (uint64_t len : b->layer_len[i]) {
+      d.layer_off.push_back(o);
+      d.layer_len.push_back(len);
+      o += len;
+    }
+    d.mats.push_back(TreeMatrix{b->d_lde[i], b->rows_of(i), b->shapes[i].width});
+    b->trees.push_back(std::move(t));
+  }
+  return ZKB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zkb_batch_create(const zkb_hasher *hasher, const zkb_batch_shape *shapes, size_t n,
+                     const zkb_batch_options *opt, zkb_batch **out) {
+  clear_error();
+  ZKB_REQUIRE(hasher && shapes && opt && out, "null arguments");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device available");
+    return ZKB_DECLINED;
+  }
+  ZKB_REQUIRE(n >= 1 && n <= (size_t)MAX_BATCH, "batch of %zu traces (1..%d)", n, MAX_BATCH);
+  auto b = std::make_unique<zkb_batch>();
+  ZKB_CHECK_CUDA(cudaGetDevice(&b->device));
+  if (!make_hasher_spec(hasher->field, (int)hasher->width, hasher->seed, &b->spec)) {
+    set_error("unsupported Poseidon2 hasher: field %d width %u", hasher->field, hasher->width);
+    return ZKB_ERR_UNSUPPORTED;
+  }
+  const int two_adicity = hasher->field == ZKB_FIELD_BABYBEAR ? 27 : 32;
+  ZKB_REQUIRE(opt->log_blowup >= 1 && opt->log_blowup <= 4, "log_blowup must be in [1, 4]");
+  for (size_t i = 0; i < n; i++)
+    ZKB_REQUIRE(shapes[i].width >= 1 && shapes[i].width <= 4096 &&
+                    (int)(shapes[i].log_h + opt->log_blowup) <= two_adicity && shapes[i].log_h <= 26,
+                "trace %zu: unsupported shape 2^%u x %u", i, shapes[i].log_h, shapes[i].width);
+  b->shapes.assign(shapes, shapes + n);
+  b->log_b = opt->log_blowup;
+  b->es = field_elem_bytes(hasher->field);
+  b->out = b->spec.out;
+  b->use_graph = opt->use_graph != 0;
+  bool ok;
+  if (b->spec.field == FIELD_BABYBEAR)
+    ok = build_p2_params<BabyBear, 16>(b->spec, &b->p_bb16);
+  else if (b->spec.width == 16)
+    ok = build_p2_params<Goldilocks, 16>(b->spec, &b->p_gl16);
+  else
+    ok = build_p2_params<Goldilocks, 12>(b->spec, &b->p_gl12);
+  ZKB_REQUIRE(ok, "invalid Poseidon2 parameters");
+  ZKB_CHECK_CUDA(cudaStreamCreateWithFlags(&b->s_main, cudaStreamNonBlocking));
+  ZKB_TRY(batch_build(b.get(), *opt));
+  *out = b.release();
+  return ZKB_OK;
+}
+
+int zkb_batch_trace_ptr(zkb_batch *b, size_t i, void **d_trace) {
+  clear_error();
+  ZKB_REQUIRE(b && d_trace && i < b->shapes.size(), "invalid trace request");
+  *d_trace = b->d_in[i];
+  return ZKB_OK;
+}
+
+int zkb_batch_copy_in(zkb_batch *b, size_t i, const void *src, int src_on_device, void *stream) {
+  clear_error();
+  ZKB_REQUIRE(b && src && i < b->shapes.size(), "invalid copy request");
+  ZKB_CHECK_CUDA(cudaSetDevice(b->device));
+  const uint64_t bytes = (1ull << b->shapes[i].log_h) * b->shapes[i].width * b->es;
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(b->d_in[i], src, bytes,
+                                 src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 resolve_stream(stream)));
+  return ZKB_OK;
+}
+
+int zkb_batch_run(zkb_batch *b, void *stream) {
+  clear_error();
+  ZKB_REQUIRE(b != nullptr, "null batch");
+  ZKB_CHECK_CUDA(cudaSetDevice(b->device));
+  return b->run(resolve_stream(stream));
+}
+
+int zkb_batch_roots(zkb_batch *b, void *roots_out, void *stream) {
+  clear_error();
+  ZKB_REQUIRE(b && roots_out, "null arguments");
+  ZKB_CHECK_CUDA(cudaSetDevice(b->device));
+  cudaStream_t s = resolve_stream(stream);
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(roots_out, b->d_roots, b->shapes.size() * b->out * b->es,
+                                 cudaMemcpyDeviceToHost, s));
+  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  return ZKB_OK;
+}
+
+int zkb_batch_tree(zkb_batch *b, size_t i, const zkb_tree **tree) {
+  clear_error();
+  ZKB_REQUIRE(b && tree && i < b->trees.size(), "invalid tree request");
+  *tree = b->trees[i].get();
+  return ZKB_OK;
+}
+
+int zkb_batch_info(const zkb_batch *b, zkb_batch_info_t *info) {
+  clear_error();
+  ZKB_REQUIRE(b && info, "null arguments");
+  info->device_bytes = b->arena_bytes;
+  info->kernels_per_run = b->use_graph ? b->kernels_per_run : 0;
+  info->branches = b->branches;
+  info->leaf_threads = b->leaf_threads;
+  info->use_graph = b->use_graph ? 1 : 0;
+  info->tuned_from_cache = b->tuned_from_cache ? 1 : 0;
+  info->tune_ms = b->tune_ms;
+  return ZKB_OK;
+}
+
+int zkb_batch_lde_tune(const zkb_batch *b, size_t i, int *kmax, uint32_t *c_pass, uint32_t *c_fused) {
+  clear_error();
+  ZKB_REQUIRE(b && i < b->tune.size() && kmax && c_pass && c_fused, "invalid request");
+  *kmax = b->tune[i].kmax;
+  *c_pass = b->tune[i].c_pass;
+  *c_fused = b->tune[i].c_fused;
+  return ZKB_OK;
+}
+
+void zkb_batch_free(zkb_batch *b) { delete b; }
+
+}  // extern "C"

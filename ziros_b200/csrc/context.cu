@@ -99,6 +99,14 @@ cudaEvent_t take_event(int dev) {
 bool profiling_enabled() { return g_prof_on; }
 
 int prof_record(const char *name, cudaStream_t s, int phase, void **token) {
+  if (phase == 0) {
+    // launches recorded into a CUDA graph are not timed one by one
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      cudaGetLastError();
+      return ZKB_OK;
+    }
+  }
   std::lock_guard<std::mutex> lk(g_prof_mu);
   if (phase == 0) {
     int dev = 0;

@@ -24,10 +24,20 @@ int p2_permute_batch(typename F::T *d_states, size_t n_states, const P2Params<F,
 // Column-wise natural-order DFT of a row-major 2^log_h x width matrix, in place.
 template <class F>
 int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaStream_t s);
+// Kernel-shape choices of one LDE (zero = default): largest pass in index bits, columns
+// per CTA of the plain passes and of the fused middle kernel.
+struct LdeTune {
+  int kmax = 0;
+  uint32_t c_pass = 0;
+  uint32_t c_fused = 0;
+};
+int lde_tune_check(int field, uint32_t width, const LdeTune &t);
 // p3 coset_lde_batch (+ bit_reverse_rows when bitrev): d_out holds 2^(log_h+log_b) rows.
+// coef_scratch (2^log_h x width), when given, is used instead of an allocation.
 template <class F>
 int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log_b,
-                typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s);
+                typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s,
+                const LdeTune *tune = nullptr, typename F::T *coef_scratch = nullptr);
 // Natural-order DFT with caller-supplied twiddle (2^log_h) and temp (2^log_h x width) buffers.
 template <class F>
 int ntt_dft_into(typename F::T *d, int log_h, uint32_t width, bool inverse, typename F::T *tw_buf,
@@ -53,6 +63,7 @@ struct DeviceTree {
   std::vector<uint64_t> layer_len;          // in digests
   std::vector<TreeMatrix> mats;             // commit order
   std::vector<void *> owned;                // device copies made by host-pointer commits
+  bool borrowed = false;                    // d_layers lives in another object's arena
   ~DeviceTree();
 };
 

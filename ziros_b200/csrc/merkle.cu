@@ -113,7 +113,7 @@ DeviceTree::~DeviceTree() {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
-  if (d_layers) cudaFreeAsync(d_layers, stream);
+  if (d_layers && !borrowed) cudaFreeAsync(d_layers, stream);
   for (void *p : owned) cudaFreeAsync(p, stream);
   cudaSetDevice(prev);
 }

@@ -381,9 +381,9 @@ template <class F>
 static int run_plan(const typename F::T *in, typename F::T *out, int L, uint32_t width,
                     uint64_t n_blocks, const typename F::T *tw, bool inverse,
                     typename F::T last_scale, const std::vector<int> &ks, int hi_start,
-                    cudaStream_t s) {
+                    cudaStream_t s, uint32_t C = 0) {
   using T = typename F::T;
-  const uint32_t C = pick_cols<F>(width);
+  if (C == 0) C = pick_cols<F>(width);
   // the register DIFs use w_64 of the same direction as the table `tw`
   const SmallTw<F> st = small_twiddles<F>(inverse);
   int hi = hi_start;
@@ -679,15 +679,42 @@ static int launch_fused_k(int K, const typename F::T *in, typename F::T *out, co
 //   lde_fused_kernel (last inverse pass + coset twists + first forward pass),
 //   the remaining forward passes in place on the 2^log_b coset blocks,
 // with the forward plan the mirror of the inverse one so both meet at K bits.
+int lde_tune_check(int field, uint32_t width, const LdeTune &t) {
+  const int kmax = field == FIELD_BABYBEAR ? 11 : 10;
+  const uint32_t cmax = field == FIELD_BABYBEAR ? 16 : 8;
+  ZKB_REQUIRE(t.kmax >= 0 && t.kmax <= kmax, "LDE tuning: pass size %d out of range", t.kmax);
+  ZKB_REQUIRE(t.c_pass == 0 || ((t.c_pass == 1 || t.c_pass == 4 || t.c_pass == 8 || t.c_pass == 16) &&
+                                t.c_pass <= cmax && width % t.c_pass == 0),
+              "LDE tuning: pass column chunk %u does not fit width %u", t.c_pass, width);
+  ZKB_REQUIRE(t.c_fused == 0 || ((t.c_fused == 1 || t.c_fused == 4 || t.c_fused == 8) && width % t.c_fused == 0),
+              "LDE tuning: fused column chunk %u does not fit width %u", t.c_fused, width);
+  return ZKB_OK;
+}
+
+// Coset LDE, rows bit-reversed (the PCS order):
+//   inverse passes over all but the lowest K bits (trace -> coefficient scratch),
+//   lde_fused_kernel (last inverse pass + coset twists + first forward pass),
+//   the remaining forward passes in place on the 2^log_b coset blocks,
+// with the forward plan the mirror of the inverse one so both meet at K bits.
+// `tune` overrides the pass size and column chunks (zero fields keep the defaults);
+// `coef_scratch` (2^log_h x width elements), when given, replaces the scratch
+// allocation, so that with bitrev set the call allocates nothing.
 template <class F>
 int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log_b,
-                typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s) {
+                typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s,
+                const LdeTune *tune, typename F::T *coef_scratch) {
   using T = typename F::T;
   if (width == 0) return ZKB_OK;
   if (log_h + log_b > F::TWO_ADICITY) {
     set_error("LDE size 2^%d exceeds the two-adicity of the field", log_h + log_b);
     return ZKB_ERR_INVALID;
   }
+  LdeTune tn;
+  if (tune) {
+    ZKB_TRY(lde_tune_check(field_id<F>(), width, *tune));
+    tn = *tune;
+  }
+  const int kmax = tn.kmax ? tn.kmax : pass_kmax<F>();
   const uint64_t n = 1ull << log_h;
   const T *ctab;
   ZKB_TRY(get_coset_table<F>(log_h, log_b, shift, &ctab, s));
@@ -698,17 +725,21 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
     const T *itw, *ftw;
     ZKB_TRY(get_twiddles<F>(log_h, true, &itw, s));
     ZKB_TRY(get_twiddles<F>(log_h, false, &ftw, s));
-    const std::vector<int> ks = plan_passes(log_h, pass_kmax<F>());
+    const std::vector<int> ks = plan_passes(log_h, kmax);
     const int Kf = ks.back();
     ScratchBuf coef;
     const T *src = d_trace;
     if (ks.size() > 1) {
-      ZKB_TRY(coef.alloc(n * width * sizeof(T), s));
+      T *cs = coef_scratch;
+      if (!cs) {
+        ZKB_TRY(coef.alloc(n * width * sizeof(T), s));
+        cs = coef.as<T>();
+      }
       std::vector<int> head(ks.begin(), ks.end() - 1);
-      ZKB_TRY(run_plan<F>(d_trace, coef.as<T>(), log_h, width, 1, itw, true, (T)0, head, log_h, s));
-      src = coef.as<T>();
+      ZKB_TRY(run_plan<F>(d_trace, cs, log_h, width, 1, itw, true, (T)0, head, log_h, s, tn.c_pass));
+      src = cs;
     }
-    const uint32_t Cf = width % 8 == 0 ? 8 : (width % 4 == 0 ? 4 : 1);
+    const uint32_t Cf = tn.c_fused ? tn.c_fused : (width % 8 == 0 ? 8 : (width % 4 == 0 ? 4 : 1));
     FusedGeom g;
     g.L = log_h;
     g.width = width;
@@ -724,7 +755,7 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
     std::vector<int> tail(ks.rbegin() + 1, ks.rend());
     if (!tail.empty())
       ZKB_TRY(run_plan<F>(d_out, d_out, log_h, width, 1ull << log_b, ftw, false, (T)0, tail,
-                          log_h - Kf, s));
+                          log_h - Kf, s, tn.c_pass));
   }
   if (!bitrev) {
     const int LN = log_h + log_b;
@@ -764,8 +795,8 @@ template int get_twiddles<Goldilocks>(int, bool, const uint64_t **, cudaStream_t
 template int ntt_dft_dev<BabyBear>(uint32_t *, int, uint32_t, bool, cudaStream_t);
 template int ntt_dft_dev<Goldilocks>(uint64_t *, int, uint32_t, bool, cudaStream_t);
 template int ntt_lde_dev<BabyBear>(const uint32_t *, int, uint32_t, int, uint32_t, bool, uint32_t *,
-                                   cudaStream_t);
+                                   cudaStream_t, const LdeTune *, uint32_t *);
 template int ntt_lde_dev<Goldilocks>(const uint64_t *, int, uint32_t, int, uint64_t, bool,
-                                     uint64_t *, cudaStream_t);
+                                     uint64_t *, cudaStream_t, const LdeTune *, uint64_t *);
 
 }  // namespace zkb
