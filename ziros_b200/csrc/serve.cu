@@ -152,8 +152,17 @@ int zkb_engine_create(const zkb_engine_config *cfg, zkb_engine **out) {
   ZKB_CHECK_CUDA(cudaGetDevice(&e->device));
   size_t free_b = 0, total_b = 0;
   ZKB_CHECK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  // memory this process's pool keeps after earlier jobs is free for the engine's jobs too
+  uint64_t pool_idle = 0;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, e->device) == cudaSuccess) {
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+      pool_idle = reserved - used;
+  }
   const uint64_t reserve = 2ull << 30;
-  const uint64_t avail = free_b > reserve ? free_b - reserve : 0;
+  const uint64_t avail = free_b + pool_idle > reserve ? free_b + pool_idle - reserve : 0;
   e->budget = cfg->hbm_budget ? (cfg->hbm_budget < avail ? cfg->hbm_budget : avail) : avail;
   zkb_engine *raw = e.get();
   for (uint32_t i = 0; i < cfg->slots; i++) e->workers.emplace_back([raw] { raw->worker_loop(); });
