@@ -30,115 +30,15 @@
 
 #include "common.cuh"
 #include "engine.cuh"
+#include "multitree.cuh"
 #include "poseidon2.cuh"
 
 namespace zkb {
 namespace {
 
 constexpr int MAX_BATCH = 1024;
-
-struct LeafJob {
-  const void *lde;     // N x width, row-major, bit-reversed rows
-  void *digests;       // N x OUT
-  uint64_t row_start;  // prefix over the jobs
-  uint64_t rows;
-  uint64_t width;
-};
-
-struct CompJob {
-  const void *prev;  // 2 * n_out digests
-  void *next;        // n_out digests
-  uint64_t start;    // prefix over the jobs of one level
-  uint64_t n_out;
-};
-
-template <int W>
-constexpr int digest_len() {
-  return W == 16 ? 8 : 4;
-}
-
-// index of the last job whose start <= g (starts ascending, starts[0] = 0)
-__device__ __forceinline__ int find_job(const uint64_t *starts, int n, uint64_t g) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (starts[mid] <= g)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
-
-// PaddingFreeSponge leaf digest of every row of every job (one permutation call site).
-template <class F, int W>
-__global__ void __launch_bounds__(256)
-    batch_leaf_kernel(const LeafJob *__restrict__ jobs, int n_jobs, uint64_t total_rows,
-                      const __grid_constant__ P2Params<F, W> p) {
-  using T = typename F::T;
-  using D = Dom<F>;
-  constexpr int OUT = digest_len<W>();
-  extern __shared__ uint64_t starts[];  // n_jobs entries
-  for (int i = threadIdx.x; i < n_jobs; i += blockDim.x) starts[i] = jobs[i].row_start;
-  __syncthreads();
-  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total_rows;
-       g += (uint64_t)gridDim.x * blockDim.x) {
-    const int j = find_job(starts, n_jobs, g);
-    const uint64_t row = g - starts[j];
-    const uint64_t width = jobs[j].width;
-    const T *rp = (const T *)jobs[j].lde + row * width;
-    T s[W];
-#pragma unroll
-    for (int i = 0; i < W; i++) s[i] = 0;
-    for (uint64_t c = 0; c < width; c += 8) {
-#pragma unroll
-      for (int i = 0; i < 8; i++)
-        if (c + i < width) s[i] = D::enter(rp[c + i]);
-      p2_permute<F, W>(s, p);
-    }
-    T *out = (T *)jobs[j].digests + row * OUT;
-#pragma unroll
-    for (int i = 0; i < OUT; i++) out[i] = D::leave(s[i]);
-  }
-}
-
-// next[i] = compress(prev[2i], prev[2i+1]) for every job of one tree level.
-template <class F, int W>
-__global__ void __launch_bounds__(128)
-    batch_compress_kernel(const CompJob *__restrict__ jobs, int n_jobs, uint64_t total,
-                          const __grid_constant__ P2Params<F, W> p) {
-  using T = typename F::T;
-  using D = Dom<F>;
-  constexpr int OUT = digest_len<W>();
-  extern __shared__ uint64_t starts[];  // n_jobs entries
-  for (int i = threadIdx.x; i < n_jobs; i += blockDim.x) starts[i] = jobs[i].start;
-  __syncthreads();
-  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
-       g += (uint64_t)gridDim.x * blockDim.x) {
-    const int j = find_job(starts, n_jobs, g);
-    const uint64_t i = g - starts[j];
-    const T *prev = (const T *)jobs[j].prev;
-    T s[W];
-#pragma unroll
-    for (int k = 0; k < OUT; k++) {
-      s[k] = D::enter(prev[(2 * i) * OUT + k]);
-      s[OUT + k] = D::enter(prev[(2 * i + 1) * OUT + k]);
-    }
-#pragma unroll
-    for (int k = 2 * OUT; k < W; k++) s[k] = 0;
-    p2_permute<F, W>(s, p);
-    T *next = (T *)jobs[j].next + i * OUT;
-#pragma unroll
-    for (int k = 0; k < OUT; k++) next[k] = D::leave(s[k]);
-  }
-}
-
-template <class T, int OUT>
-__global__ void batch_roots_kernel(const uint64_t *__restrict__ root_off, const T *__restrict__ digests,
-                                   int n, T *__restrict__ roots) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n * OUT) roots[t] = digests[root_off[t / OUT] * OUT + (t % OUT)];
-}
+using mt::CompJob;
+using mt::LeafJob;
 
 uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
 
@@ -213,16 +113,13 @@ struct zkb_batch {
   void *arena = nullptr;
   uint64_t arena_bytes = 0;
   std::vector<void *> d_in, d_lde, d_layers;
-  std::vector<std::vector<uint64_t>> layer_len;  // per trace, in digests
   std::vector<void *> d_coef;                    // per branch: scratch for its largest trace
   uint64_t coef_bytes = 0;
   void *d_roots = nullptr;
   uint64_t *d_root_off = nullptr;  // digest offsets of the roots from d_layers[0]
   LeafJob *d_leaf_jobs = nullptr;
   CompJob *d_comp_jobs = nullptr;
-  uint64_t total_rows = 0;
-  std::vector<size_t> lvl_off, lvl_cnt;
-  std::vector<uint64_t> lvl_total;
+  mt::Tables tables;
   // kernel shapes
   std::vector<LdeTune> tune;  // per trace
   unsigned leaf_threads = 128;
@@ -280,17 +177,8 @@ struct zkb_batch {
 
   template <class F, int W>
   int hash_all(const P2Params<F, W> &p, unsigned threads, cudaStream_t s) {
-    DeviceContext *ctx;
-    ZKB_TRY(current_context(&ctx));
-    const int n = (int)shapes.size();
-    ZKB_LAUNCH("batch_leaf_hash", s, batch_leaf_kernel<F, W><<<grid_for(total_rows, threads, (unsigned)ctx->sm_count * (2048u / threads)), threads, n * sizeof(uint64_t), s>>>(d_leaf_jobs, n, total_rows, p));
-    for (size_t l = 0; l < lvl_cnt.size(); l++) {
-      ZKB_LAUNCH("batch_compress", s, batch_compress_kernel<F, W><<<grid_for(lvl_total[l], 128, (unsigned)ctx->sm_count * 16u), 128, lvl_cnt[l] * sizeof(uint64_t), s>>>(d_comp_jobs + lvl_off[l], (int)lvl_cnt[l], lvl_total[l], p));
-    }
-    using T = typename F::T;
-    constexpr int OUT = digest_len<W>();
-    ZKB_LAUNCH("batch_roots", s, batch_roots_kernel<T, OUT><<<(n * OUT + 127) / 128, 128, 0, s>>>(d_root_off, (const T *)d_layers[0], n, (T *)d_roots));
-    return ZKB_OK;
+    return mt::launch_trees<F, W>(tables, d_leaf_jobs, d_comp_jobs, d_root_off, d_layers[0], d_roots, p, threads, s,
+                                  "batch_leaf_hash", "batch_compress", "batch_roots");
   }
 
   int hash_dispatch(unsigned threads, cudaStream_t s) {
@@ -605,15 +493,11 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   off = align256(off + total_digests * OUT * es);
   const uint64_t roots_off = off;
   off = align256(off + n * OUT * es);
-  const uint64_t root_off_off = off;
-  off = align256(off + n * 8);
-  const uint64_t leaf_jobs_off = off;
-  off = align256(off + n * sizeof(LeafJob));
-  // compression levels: level l exists for trace i when N_i > 2^l
-  int max_levels = 0;
-  for (size_t i = 0; i < n; i++) max_levels = std::max<int>(max_levels, (int)(b->shapes[i].log_h + b->log_b));
-  const uint64_t comp_jobs_off = off;
-  off = align256(off + (uint64_t)max_levels * n * sizeof(CompJob));
+  // job tables: n leaf jobs, one compression job per level of every tree, n root offsets
+  uint64_t n_comp = 0;
+  for (size_t i = 0; i < n; i++) n_comp += b->shapes[i].log_h + b->log_b;
+  const uint64_t tables_off = off;
+  off = align256(off + n * sizeof(LeafJob) + n_comp * sizeof(CompJob) + n * 8);
   b->arena_bytes = off;
 
   size_t free_b = 0, total_b = 0;
@@ -632,49 +516,21 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
     b->d_layers[i] = base + layers_base + lay_off[i] * OUT * es;
   }
   b->d_roots = base + roots_off;
-  b->d_root_off = (uint64_t *)(base + root_off_off);
-  b->d_leaf_jobs = (LeafJob *)(base + leaf_jobs_off);
-  b->d_comp_jobs = (CompJob *)(base + comp_jobs_off);
 
   // ---- job tables
-  std::vector<LeafJob> leaf(n);
-  std::vector<uint64_t> root_off(n);
-  uint64_t rs = 0;
-  b->layer_len.assign(n, {});
+  std::vector<const void *> data(n);
+  std::vector<uint64_t> rows(n), widths(n);
   for (size_t i = 0; i < n; i++) {
-    const uint64_t N = b->rows_of(i);
-    leaf[i] = LeafJob{b->d_lde[i], b->d_layers[i], rs, N, b->shapes[i].width};
-    rs += N;
-    uint64_t o = 0;
-    for (uint64_t len = N;; len /= 2) {
-      b->layer_len[i].push_back(len);
-      if (len == 1) break;
-      o += len;
-    }
-    root_off[i] = lay_off[i] + o;
+    data[i] = b->d_lde[i];
+    rows[i] = b->rows_of(i);
+    widths[i] = b->shapes[i].width;
   }
-  b->total_rows = rs;
-  std::vector<CompJob> comp;
-  for (int l = 0; l < max_levels; l++) {
-    b->lvl_off.push_back(comp.size());
-    uint64_t start = 0;
-    for (size_t i = 0; i < n; i++) {
-      const auto &ll = b->layer_len[i];
-      if ((size_t)l + 1 >= ll.size()) continue;
-      uint64_t lo = 0;
-      for (int q = 0; q < l; q++) lo += ll[q];
-      const char *lay = (const char *)b->d_layers[i];
-      comp.push_back(CompJob{lay + lo * OUT * es, (void *)(lay + (lo + ll[l]) * OUT * es), start, ll[l] / 2});
-      start += ll[l] / 2;
-    }
-    b->lvl_cnt.push_back(comp.size() - b->lvl_off.back());
-    b->lvl_total.push_back(start);
-  }
+  mt::build_tables(data, rows, widths, b->d_layers, b->d_layers[0], OUT, es, &b->tables);
+  ZKB_REQUIRE(b->tables.device_bytes() <= n * sizeof(LeafJob) + n_comp * sizeof(CompJob) + n * 8,
+              "internal: batch job tables");
   ZKB_CHECK_CUDA(cudaMemsetAsync(b->arena, 0, layers_base, b->s_main));
-  ZKB_CHECK_CUDA(cudaMemcpyAsync(b->d_leaf_jobs, leaf.data(), n * sizeof(LeafJob), cudaMemcpyHostToDevice, b->s_main));
-  ZKB_CHECK_CUDA(cudaMemcpyAsync(b->d_comp_jobs, comp.data(), comp.size() * sizeof(CompJob), cudaMemcpyHostToDevice,
-                                 b->s_main));
-  ZKB_CHECK_CUDA(cudaMemcpyAsync(b->d_root_off, root_off.data(), n * 8, cudaMemcpyHostToDevice, b->s_main));
+  ZKB_TRY(mt::upload_tables(b->tables, base + tables_off, b->s_main, &b->d_leaf_jobs, &b->d_comp_jobs,
+                            &b->d_root_off));
   ZKB_CHECK_CUDA(cudaStreamSynchronize(b->s_main));
 
   // ---- streams and events
@@ -723,7 +579,7 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
     d.d_layers = b->d_layers[i];
     d.borrowed = true;
     uint64_t o = 0;
-    for (uint64_t len : b->layer_len[i]) {
+    for (uint64_t len : b->tables.layer_len[i]) {
       d.layer_off.push_back(o);
       d.layer_len.push_back(len);
       o += len;

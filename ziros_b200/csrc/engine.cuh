@@ -86,8 +86,7 @@ struct FriProof {
   int device = 0;
   cudaStream_t stream = nullptr;
   int log_n = 0, log_final = 0;
-  std::vector<std::unique_ptr<DeviceTree>> trees;  // one per round
-  std::vector<void *> owned;                       // folded codewords (leaves of rounds >= 1)
+  std::vector<void *> owned;                       // device state: folded codewords, layer trees
   std::vector<std::array<uint32_t, 4>> betas;
   std::vector<uint32_t> final_cw;                  // 2^log_final x 4, host
   std::vector<uint32_t> roots;                     // rounds x 8, host
@@ -95,7 +94,7 @@ struct FriProof {
   std::vector<uint32_t> query_rows;                // queries x rounds x 8
   std::vector<uint32_t> query_sibs;                // queries x sib_per_query
   uint64_t sib_per_query = 0;
-  // Frees the device buffers (trees, folded codewords); host answers stay.
+  // Frees the device buffers (folded codewords, layer trees); host answers stay.
   void release_device();
   ~FriProof();
 };

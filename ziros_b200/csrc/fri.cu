@@ -12,6 +12,7 @@
 
 #include "common.cuh"
 #include "engine.cuh"
+#include "multitree.cuh"
 #include "field.cuh"
 
 namespace zkb {
@@ -212,7 +213,6 @@ void FriProof::release_device() {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
-  trees.clear();
   for (void *p : owned) cudaFreeAsync(p, stream);
   owned.clear();
   cudaSetDevice(prev);
@@ -229,76 +229,124 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
               "need 0 <= log_final < log_n <= 27 (got %d, %d)", log_final, log_n);
   ZKB_REQUIRE(num_queries >= 0 && num_queries <= 4096, "num_queries out of range");
   ZKB_REQUIRE(((uintptr_t)d_codeword & 15) == 0, "codeword must be 16-byte aligned");
+  P2Params<BabyBear, 16> p;
+  const bool p_ok = build_p2_params<BabyBear, 16>(spec, &p);
+  ZKB_REQUIRE(p_ok, "invalid Poseidon2 parameters");
   ZKB_CHECK_CUDA(cudaGetDevice(&pf->device));
   pf->stream = s;
   pf->log_n = log_n;
   pf->log_final = log_final;
   const int rounds = log_n - log_final;
+  // The challenges are seeded draws, so every fold can run before any layer is hashed:
+  // fold all rounds, then hash the trees of all rounds together (one leaf launch, one
+  // launch per tree level across the rounds, one root gather).
   SmallRng rng(challenge_seed);
-  const uint32_t *cur = d_codeword;
-  uint64_t len = 1ull << log_n;
   for (int r = 0; r < rounds; r++) {
-    auto tree = std::make_unique<DeviceTree>();
-    std::vector<TreeMatrix> m{{cur, len / 2, 8}};
-    ZKB_TRY(mmcs_build_dev(spec, m, tree.get(), s, true));
     std::array<uint32_t, 4> beta;
     for (auto &b : beta) b = sample_babybear(rng);
     pf->betas.push_back(beta);
-    void *next = nullptr;
-    ZKB_TRY(dev_alloc(&next, (len / 2) * 16, s));
-    pf->owned.push_back(next);
-    ZKB_TRY(fri_fold_ext4_dev(cur, len / 2, beta.data(), (uint32_t *)next, s));
-    pf->trees.push_back(std::move(tree));
-    cur = (const uint32_t *)next;
-    len /= 2;
   }
-  // final codeword and per-round roots to the host
-  pf->final_cw.resize(len * 4);
-  ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->final_cw.data(), cur, len * 16, cudaMemcpyDeviceToHost, s));
-  pf->roots.resize((size_t)rounds * 8);
-  for (int r = 0; r < rounds; r++) {
-    const DeviceTree &t = *pf->trees[r];
-    ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->roots.data() + (size_t)r * 8,
-                                   (const uint32_t *)t.d_layers + t.layer_off.back() * 8, 32,
-                                   cudaMemcpyDeviceToHost, s));
-  }
-  // queries
   SmallRng qr(query_seed);
   pf->query_idx.resize(num_queries);
   for (auto &q : pf->query_idx) q = qr.next_u64() >> (64 - log_n);
-  std::vector<FriRoundDesc> descs(rounds);
-  std::vector<uint64_t> sib_off(rounds + 1, 0);
-  for (int r = 0; r < rounds; r++) {
-    const DeviceTree &t = *pf->trees[r];
-    FriRoundDesc &d = descs[r];
-    d.leaves = (const uint32_t *)t.mats[0].data;
-    d.layers = (const uint32_t *)t.d_layers;
-    d.depth = log_n - r - 1;
-    ZKB_REQUIRE(d.depth < 40 && (size_t)d.depth < t.layer_off.size(), "internal: FRI tree depth");
-    for (int l = 0; l < d.depth; l++) d.layer_off[l] = t.layer_off[l];
-    sib_off[r + 1] = sib_off[r] + (uint64_t)d.depth * 8;
+
+  // ---- one device allocation: folded codewords, digest layers, roots, tables, query answers
+  auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+  uint64_t off = 0;
+  std::vector<uint64_t> cw_off(rounds + 1, 0), lay_off(rounds);
+  for (int r = 1; r <= rounds; r++) {  // codeword of round r (round `rounds` is the final one)
+    cw_off[r] = off;
+    off = al(off + (16ull << (log_n - r)));
   }
+  const uint64_t layers_base = off;
+  uint64_t digests = 0;
+  for (int r = 0; r < rounds; r++) {
+    lay_off[r] = digests;
+    digests += 2 * (1ull << (log_n - r - 1)) - 1;
+  }
+  off = al(off + digests * 32);
+  const uint64_t roots_off = off;
+  off = al(off + (uint64_t)rounds * 32);
+  uint64_t n_comp = 0;
+  for (int r = 0; r < rounds; r++) n_comp += (uint64_t)(log_n - r - 1);
+  const uint64_t tables_off = off;
+  off = al(off + rounds * sizeof(mt::LeafJob) + n_comp * sizeof(mt::CompJob) + rounds * 8ull);
+  std::vector<uint64_t> sib_off(rounds + 1, 0);
+  for (int r = 0; r < rounds; r++) sib_off[r + 1] = sib_off[r] + (uint64_t)(log_n - r - 1) * 8;
   pf->sib_per_query = sib_off[rounds];
   pf->query_rows.resize((size_t)num_queries * rounds * 8);
   pf->query_sibs.resize((size_t)num_queries * pf->sib_per_query);
-  if (num_queries > 0 && rounds > 0) {
-    ScratchBuf d_desc, d_idx, d_off, d_rows, d_sibs;
-    ZKB_TRY(d_desc.alloc(descs.size() * sizeof(FriRoundDesc), s));
-    ZKB_TRY(d_idx.alloc(num_queries * 8, s));
-    ZKB_TRY(d_off.alloc(sib_off.size() * 8, s));
-    ZKB_TRY(d_rows.alloc(pf->query_rows.size() * 4, s));
-    ZKB_TRY(d_sibs.alloc(pf->query_sibs.size() * 4, s));
-    ZKB_CHECK_CUDA(cudaMemcpyAsync(d_desc.p, descs.data(), descs.size() * sizeof(FriRoundDesc),
+  const uint64_t desc_off = off;
+  off = al(off + rounds * sizeof(FriRoundDesc));
+  const uint64_t idx_off = off;
+  off = al(off + (uint64_t)num_queries * 8 + 8);
+  const uint64_t soff_off = off;
+  off = al(off + sib_off.size() * 8);
+  const uint64_t rows_off = off;
+  off = al(off + pf->query_rows.size() * 4 + 4);
+  const uint64_t sibs_off = off;
+  off = al(off + pf->query_sibs.size() * 4 + 4);
+  void *arena = nullptr;
+  ZKB_TRY(dev_alloc(&arena, off, s));
+  pf->owned.push_back(arena);
+  char *base = (char *)arena;
+  auto cw = [&](int r) -> const uint32_t * {
+    return r == 0 ? d_codeword : (const uint32_t *)(base + cw_off[r]);
+  };
+
+  // ---- folds
+  for (int r = 0; r < rounds; r++)
+    ZKB_TRY(fri_fold_ext4_dev(cw(r), 1ull << (log_n - r - 1), pf->betas[r].data(), (uint32_t *)cw(r + 1), s));
+
+  // ---- trees of every round: round r commits 2^(log_n-r-1) rows of 8 (sibling pairs)
+  std::vector<const void *> data(rounds);
+  std::vector<uint64_t> rows(rounds), widths(rounds, 8);
+  std::vector<void *> layers(rounds);
+  for (int r = 0; r < rounds; r++) {
+    data[r] = cw(r);
+    rows[r] = 1ull << (log_n - r - 1);
+    layers[r] = base + layers_base + lay_off[r] * 32;
+  }
+  mt::Tables tab;
+  mt::build_tables(data, rows, widths, layers, layers[0], 8, 4, &tab);
+  mt::LeafJob *d_leaf;
+  mt::CompJob *d_comp;
+  uint64_t *d_root_off;
+  ZKB_TRY(mt::upload_tables(tab, base + tables_off, s, &d_leaf, &d_comp, &d_root_off));
+  ZKB_TRY((mt::launch_trees<BabyBear, 16>(tab, d_leaf, d_comp, d_root_off, layers[0], base + roots_off, p, 128, s,
+                                          "fri_leaf_hash", "fri_compress", "fri_roots")));
+
+  // ---- answers to the host: roots, final codeword, query openings
+  pf->roots.resize((size_t)rounds * 8);
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->roots.data(), base + roots_off, (size_t)rounds * 32, cudaMemcpyDeviceToHost, s));
+  pf->final_cw.resize((1ull << log_final) * 4);
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->final_cw.data(), cw(rounds), 16ull << log_final, cudaMemcpyDeviceToHost, s));
+  if (num_queries > 0) {
+    std::vector<FriRoundDesc> descs(rounds);
+    for (int r = 0; r < rounds; r++) {
+      FriRoundDesc &d = descs[r];
+      d.leaves = cw(r);
+      d.layers = (const uint32_t *)layers[r];
+      d.depth = log_n - r - 1;
+      ZKB_REQUIRE(d.depth < 40, "internal: FRI tree depth");
+      uint64_t o = 0;
+      for (int l = 0; l < d.depth; l++) {
+        d.layer_off[l] = o;
+        o += tab.layer_len[r][l];
+      }
+    }
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(base + desc_off, descs.data(), descs.size() * sizeof(FriRoundDesc),
                                    cudaMemcpyHostToDevice, s));
-    ZKB_CHECK_CUDA(cudaMemcpyAsync(d_idx.p, pf->query_idx.data(), num_queries * 8, cudaMemcpyHostToDevice, s));
-    ZKB_CHECK_CUDA(cudaMemcpyAsync(d_off.p, sib_off.data(), sib_off.size() * 8, cudaMemcpyHostToDevice, s));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(base + idx_off, pf->query_idx.data(), num_queries * 8, cudaMemcpyHostToDevice, s));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(base + soff_off, sib_off.data(), sib_off.size() * 8, cudaMemcpyHostToDevice, s));
     const int tasks = num_queries * rounds;
-    ZKB_LAUNCH("fri_query_gather", s, fri_gather_kernel<<<(tasks + 127) / 128, 128, 0, s>>>(d_desc.as<FriRoundDesc>(), rounds, d_idx.as<uint64_t>(), num_queries, d_rows.as<uint32_t>(), d_sibs.as<uint32_t>(), d_off.as<uint64_t>()));
-    ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->query_rows.data(), d_rows.p, pf->query_rows.size() * 4,
+    ZKB_LAUNCH("fri_query_gather", s, fri_gather_kernel<<<(tasks + 127) / 128, 128, 0, s>>>((const FriRoundDesc *)(base + desc_off), rounds, (const uint64_t *)(base + idx_off), num_queries, (uint32_t *)(base + rows_off), (uint32_t *)(base + sibs_off), (const uint64_t *)(base + soff_off)));
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->query_rows.data(), base + rows_off, pf->query_rows.size() * 4,
                                    cudaMemcpyDeviceToHost, s));
-    ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->query_sibs.data(), d_sibs.p, pf->query_sibs.size() * 4,
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->query_sibs.data(), base + sibs_off, pf->query_sibs.size() * 4,
                                    cudaMemcpyDeviceToHost, s));
   }
+  // the host tables above must outlive their (staged) uploads; the answers must be on the host
   ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
   return ZKB_OK;
 }
