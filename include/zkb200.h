@@ -149,8 +149,9 @@ ZKB_API int zkb_coset_lde_batch_dev(int field, const void *d_trace, uint32_t log
                             void *stream);
 /* The device LDE (generator shift, bit-reversed rows) with explicit kernel shapes:
  * largest NTT pass kmax index bits (1..11 BabyBear, 1..10 Goldilocks; 0 = default) and
- * columns per CTA of the plain passes (1/4/8/16, 0 = default) and of the fused middle
- * kernel (1/4/8, 0 = default).  Every choice gives the same output; the batched plan's
+ * the widest column chunk per CTA of the plain passes (1/4/8/16, 0 = default) and of the
+ * fused middle kernel (1/4/8, 0 = default); columns beyond a multiple of the chunk take
+ * narrower chunks.  Every choice gives the same output; the batched plan's
  * autotuner picks among them.  No counterpart in the reference (its Metal NTT has one
  * fixed dispatch shape, zkf-metal/src/ntt/p3_adapter.rs:78-294). */
 ZKB_API int zkb_coset_lde_tuned_dev(int field, const void *d_trace, uint32_t log_h, uint32_t width,

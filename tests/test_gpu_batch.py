@@ -134,7 +134,7 @@ def test_tune_cache_roundtrip(tmp_path):
 
 
 @pytest.mark.parametrize("field,log_h,width", [(Z.BABYBEAR, 14, 48), (Z.BABYBEAR, 20, 16), (Z.GOLDILOCKS, 13, 24),
-                                               (Z.BABYBEAR, 9, 7)])
+                                               (Z.BABYBEAR, 9, 7), (Z.BABYBEAR, 12, 415), (Z.GOLDILOCKS, 11, 29)])
 def test_every_lde_kernel_shape_gives_the_same_lde(field, log_h, width):
     """The autotuner's candidates (pass split, column chunks) are all the same function."""
     import torch
@@ -148,7 +148,7 @@ def test_every_lde_kernel_shape_gives_the_same_lde(field, log_h, width):
     for kmax in (kdef, kdef - 1, kdef - 2, 5, 3):
         for cp in (16, 8, 4, 1):
             for cf in (8, 4, 1):
-                if width % cp or width % cf or (field == Z.GOLDILOCKS and cp == 16):
+                if field == Z.GOLDILOCKS and cp == 16:
                     continue
                 out = torch.empty_like(ref)
                 dft.coset_lde_tuned_dev(tt, 1, out, kmax, cp, cf)

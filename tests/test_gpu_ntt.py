@@ -35,7 +35,7 @@ def test_dft_known_answer():
 
 
 @pytest.mark.parametrize("field", [Z.BABYBEAR, Z.GOLDILOCKS])
-@pytest.mark.parametrize("seed,width", [(5, 1), (23, 4), (0, 16)])
+@pytest.mark.parametrize("seed,width", [(5, 1), (23, 4), (0, 16), (0, 27)])
 def test_dft_matches_oracle(oracle, field, seed, width):
     m = patterned(field, 1 << 13, width, seed) if seed else rand_field(field, (1 << 13, width), 3)
     dft = Z.CudaDft(field)
@@ -55,7 +55,9 @@ def test_dft_sizes(oracle, field, log_h):
 @pytest.mark.parametrize("field", [Z.BABYBEAR, Z.GOLDILOCKS])
 @pytest.mark.parametrize("log_h,width,log_b", [
     (0, 3, 1), (1, 1, 1), (3, 5, 3), (5, 7, 2), (10, 16, 1), (13, 8, 2), (14, 16, 1), (12, 24, 3),
-    (16, 2, 1)])
+    (16, 2, 1),
+    # widths that are not a multiple of the column chunk: bulk + 8/4/1-column remainders
+    (12, 31, 1), (13, 29, 1), (11, 45, 2), (15, 13, 1)])
 def test_coset_lde_matches_oracle(oracle, field, log_h, width, log_b):
     t = rand_field(field, (1 << log_h, width), 1000 + log_h * 10 + log_b)
     got = Z.CudaDft(field).coset_lde_batch(t, log_b, bit_reverse_rows=True)

@@ -311,12 +311,25 @@ __global__ void __launch_bounds__(C << LR2)
   }
 }
 
-template <class F>
-static uint32_t pick_cols(uint32_t width) {
-  if (sizeof(typename F::T) == 4 && width % 16 == 0) return 16;
-  if (width % 8 == 0) return 8;
-  if (width % 4 == 0) return 4;
-  return 1;
+// Column segments of a `width`-column matrix: the widest chunk (at most cmax columns per
+// CTA) for the bulk, then narrower chunks (8, 4, 1) for what is left, each launched on
+// offset pointers with the full row stride.  Every width keeps coalesced rows for all
+// but at most cmax - 1 columns.
+struct ColSeg {
+  uint32_t col0, cols, C;
+};
+static std::vector<ColSeg> col_segments(uint32_t width, uint32_t cmax) {
+  std::vector<ColSeg> v;
+  uint32_t c0 = 0;
+  for (uint32_t C : {16u, 8u, 4u, 1u}) {
+    if (C > cmax) continue;
+    const uint32_t n = (width - c0) / C;
+    if (n) {
+      v.push_back(ColSeg{c0, n * C, C});
+      c0 += n * C;
+    }
+  }
+  return v;
 }
 
 // Split L bits into passes of at most kmax bits, as even as possible, top first.
@@ -381,9 +394,10 @@ template <class F>
 static int run_plan(const typename F::T *in, typename F::T *out, int L, uint32_t width,
                     uint64_t n_blocks, const typename F::T *tw, bool inverse,
                     typename F::T last_scale, const std::vector<int> &ks, int hi_start,
-                    cudaStream_t s, uint32_t C = 0) {
+                    cudaStream_t s, uint32_t cmax = 0) {
   using T = typename F::T;
-  if (C == 0) C = pick_cols<F>(width);
+  if (cmax == 0) cmax = sizeof(T) == 4 ? 16 : 8;
+  const std::vector<ColSeg> segs = col_segments(width, cmax);
   // the register DIFs use w_64 of the same direction as the table `tw`
   const SmallTw<F> st = small_twiddles<F>(inverse);
   int hi = hi_start;
@@ -394,37 +408,47 @@ static int run_plan(const typename F::T *in, typename F::T *out, int L, uint32_t
     g.L = L;
     g.lo = hi - K;
     g.width = width;
-    g.chunks_per_row = width / C;
     g.groups = 1u << (L - K);
     g.block_stride = ((uint64_t)width) << L;
     g.twist = g.lo > 0;
-    const uint64_t ctas = (uint64_t)g.chunks_per_row * g.groups * n_blocks;
-    if (ctas >= (1ull << 31) || ((uint64_t)width << L) * n_blocks >= (1ull << 40)) {
+    if (((uint64_t)width << L) * n_blocks >= (1ull << 40)) {
       set_error("NTT launch too large");
       return ZKB_ERR_UNSUPPORTED;
     }
     const T scale = (pi + 1 == ks.size()) ? last_scale : (T)0;
-    int rc;
-    switch (K) {
-      case 1: rc = launch_pass<F, 1, 0>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 2: rc = launch_pass<F, 1, 1>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 3: rc = launch_pass<F, 2, 1>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 4: rc = launch_pass<F, 2, 2>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 5: rc = launch_pass<F, 3, 2>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 6: rc = launch_pass<F, 3, 3>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 7: rc = launch_pass<F, 4, 3>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 8: rc = launch_pass<F, 4, 4>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 9: rc = launch_pass<F, 5, 4>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 10: rc = launch_pass<F, 5, 5>(src, out, g, ctas, tw, scale, st, C, s); break;
-      case 11:
-        if constexpr (sizeof(T) == 4) {
-          rc = launch_pass<F, 6, 5>(src, out, g, ctas, tw, scale, st, C, s);
-          break;
-        }
-        [[fallthrough]];
-      default:
-        set_error("internal: NTT pass of %d bits", K);
-        return ZKB_ERR_INTERNAL;
+    int rc = ZKB_OK;
+    for (const ColSeg &sg : segs) {
+      const uint32_t C = sg.C;
+      const T *sp = src + sg.col0;
+      T *op = out + sg.col0;
+      g.chunks_per_row = sg.cols / C;
+      const uint64_t ctas = (uint64_t)g.chunks_per_row * g.groups * n_blocks;
+      if (ctas >= (1ull << 31)) {
+        set_error("NTT launch too large");
+        return ZKB_ERR_UNSUPPORTED;
+      }
+      switch (K) {
+        case 1: rc = launch_pass<F, 1, 0>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 2: rc = launch_pass<F, 1, 1>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 3: rc = launch_pass<F, 2, 1>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 4: rc = launch_pass<F, 2, 2>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 5: rc = launch_pass<F, 3, 2>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 6: rc = launch_pass<F, 3, 3>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 7: rc = launch_pass<F, 4, 3>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 8: rc = launch_pass<F, 4, 4>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 9: rc = launch_pass<F, 5, 4>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 10: rc = launch_pass<F, 5, 5>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 11:
+          if constexpr (sizeof(T) == 4) {
+            rc = launch_pass<F, 6, 5>(sp, op, g, ctas, tw, scale, st, C, s);
+            break;
+          }
+          [[fallthrough]];
+        default:
+          set_error("internal: NTT pass of %d bits", K);
+          return ZKB_ERR_INTERNAL;
+      }
+      ZKB_TRY(rc);
     }
     ZKB_TRY(rc);
     src = out;
@@ -683,11 +707,12 @@ int lde_tune_check(int field, uint32_t width, const LdeTune &t) {
   const int kmax = field == FIELD_BABYBEAR ? 11 : 10;
   const uint32_t cmax = field == FIELD_BABYBEAR ? 16 : 8;
   ZKB_REQUIRE(t.kmax >= 0 && t.kmax <= kmax, "LDE tuning: pass size %d out of range", t.kmax);
+  (void)width;  // widths that are not a multiple of the chunk take narrower chunks for the rest
   ZKB_REQUIRE(t.c_pass == 0 || ((t.c_pass == 1 || t.c_pass == 4 || t.c_pass == 8 || t.c_pass == 16) &&
-                                t.c_pass <= cmax && width % t.c_pass == 0),
-              "LDE tuning: pass column chunk %u does not fit width %u", t.c_pass, width);
-  ZKB_REQUIRE(t.c_fused == 0 || ((t.c_fused == 1 || t.c_fused == 4 || t.c_fused == 8) && width % t.c_fused == 0),
-              "LDE tuning: fused column chunk %u does not fit width %u", t.c_fused, width);
+                                t.c_pass <= cmax),
+              "LDE tuning: pass column chunk %u not in {1, 4, 8, 16} (at most %u)", t.c_pass, cmax);
+  ZKB_REQUIRE(t.c_fused == 0 || t.c_fused == 1 || t.c_fused == 4 || t.c_fused == 8,
+              "LDE tuning: fused column chunk %u not in {1, 4, 8}", t.c_fused);
   return ZKB_OK;
 }
 
@@ -739,19 +764,20 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
       ZKB_TRY(run_plan<F>(d_trace, cs, log_h, width, 1, itw, true, (T)0, head, log_h, s, tn.c_pass));
       src = cs;
     }
-    const uint32_t Cf = tn.c_fused ? tn.c_fused : (width % 8 == 0 ? 8 : (width % 4 == 0 ? 4 : 1));
     FusedGeom g;
     g.L = log_h;
     g.width = width;
-    g.chunks_per_row = width / Cf;
     g.blocks = 1u << (log_h - Kf);
     g.log_b = log_b;
     g.n = n;
-    if ((uint64_t)g.chunks_per_row * g.blocks >= (1ull << 31)) {
-      set_error("LDE launch too large");
-      return ZKB_ERR_UNSUPPORTED;
+    for (const ColSeg &sg : col_segments(width, tn.c_fused ? tn.c_fused : 8)) {
+      g.chunks_per_row = sg.cols / sg.C;
+      if ((uint64_t)g.chunks_per_row * g.blocks >= (1ull << 31)) {
+        set_error("LDE launch too large");
+        return ZKB_ERR_UNSUPPORTED;
+      }
+      ZKB_TRY(launch_fused_k<F>(Kf, src + sg.col0, d_out + sg.col0, g, itw, ftw, ctab, sg.C, s));
     }
-    ZKB_TRY(launch_fused_k<F>(Kf, src, d_out, g, itw, ftw, ctab, Cf, s));
     std::vector<int> tail(ks.rbegin() + 1, ks.rend());
     if (!tail.empty())
       ZKB_TRY(run_plan<F>(d_out, d_out, log_h, width, 1ull << log_b, ftw, false, (T)0, tail,
