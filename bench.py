@@ -202,6 +202,51 @@ def run_reference(args, wl: dict, rank: int, world: int) -> int:
     return 0
 
 
+# ------------------------------------------------------------ ranks
+class Ranks:
+    """One process per GPU: the process group (NCCL on GPUs, gloo for the CPU tests),
+    the barrier around timed regions and the max over ranks of a duration.  Replicas
+    exchange nothing else: no data-path collective."""
+
+    def __init__(self, world: int, device, backend: str = "nccl", timeout_s: int = 300):
+        import torch
+
+        self.torch = torch
+        self.world = world
+        self.device = device
+        self.dist = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+        if self.device.type == "cuda":
+            self.torch.cuda.synchronize()
+
+    def max(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def whole_job_rate(units_per_rank: float, steps: int, world: int, t_max: float) -> float:
+    """Units all ranks processed / the slowest rank's time (weak scaling)."""
+    return units_per_rank * steps * world / t_max
+
+
 # ------------------------------------------------------------ GPU arm
 def make_trace(torch, wl: dict, device):
     g = torch.Generator(device=device)
@@ -266,25 +311,9 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     N.check(N.load().zkb_set_device(local_rank))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world, dev, "nccl")
+    dist = ranks.dist
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     field, lb = wl["field"], wl["log_blowup"]
     n, w = 1 << wl["log_h"], wl["width"]
@@ -361,7 +390,7 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
             dist.destroy_process_group()
         return 0
 
-    value = cells * args.steps * world / t_dev
+    value = whole_job_rate(cells, args.steps, world, t_dev)
     rounds = wl["log_h"] + lb - FRI["log_final"]
     fri_d2h = 4 * (8 * rounds + 4 * rounds + 4 * (1 << FRI["log_final"]) + FRI["num_queries"] * (
         2 + 8 * rounds + 8 * sum(wl["log_h"] + lb - r - 1 for r in range(rounds))))
@@ -470,25 +499,9 @@ def run_batch(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     dev = torch.device("cuda", local_rank)
     lib = N.load()
     N.check(lib.zkb_set_device(local_rank))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world, dev, "nccl")
+    dist = ranks.dist
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     field, lb, p2w = wl["field"], wl["log_blowup"], wl["p2w"]
     shapes = batch_shapes(wl)
@@ -591,7 +604,7 @@ def run_batch(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     for h, w in shapes:
         lp, cp = perms_of_commit((h << lb).bit_length() - 1, w)
         muls += (lp + cp) * p2_field_muls(field, p2w)
-    value = cells * args.steps * world / t_batch
+    value = whole_job_rate(cells, args.steps, world, t_batch)
     plain = cells * args.steps * world / t_plain
     ach = muls * args.steps / t_batch / 1e9
     cpu = None

@@ -340,13 +340,17 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
   void *lde = nullptr;
   ZKB_TRY(dev_alloc(&lde, N * width * es, s));
   tree->t.owned.push_back(lde);
+  // A staged copy of a host trace is ours: the inverse passes run in place on it
+  // instead of in a separate coefficient scratch.
   int rc;
   if (spec.field == FIELD_BABYBEAR)
     rc = ntt_lde_dev<BabyBear>((const uint32_t *)d_trace, (int)log_h, width, (int)log_blowup,
-                               BabyBear::GENERATOR, true, (uint32_t *)lde, s);
+                               BabyBear::GENERATOR, true, (uint32_t *)lde, s, nullptr,
+                               h_trace ? staged.as<uint32_t>() : nullptr);
   else
     rc = ntt_lde_dev<Goldilocks>((const uint64_t *)d_trace, (int)log_h, width, (int)log_blowup,
-                                 Goldilocks::GENERATOR, true, (uint64_t *)lde, s);
+                                 Goldilocks::GENERATOR, true, (uint64_t *)lde, s, nullptr,
+                                 h_trace ? staged.as<uint64_t>() : nullptr);
   ZKB_TRY(rc);
   std::vector<TreeMatrix> mats{{lde, N, width}};
   ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));

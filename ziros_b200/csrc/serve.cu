@@ -63,8 +63,7 @@ struct Job {
 uint64_t job_bytes(const zkb_job_desc &d) {
   const uint64_t es = d.hasher.field == ZKB_FIELD_BABYBEAR ? 4 : 8;
   const uint64_t n = 1ull << d.log_h, N = n << d.log_blowup;
-  uint64_t b = n * d.width * es        // staged trace
-               + n * d.width * es      // coefficient scratch of the inverse pass
+  uint64_t b = n * d.width * es        // staged trace (the inverse passes run in place on it)
                + N * d.width * es      // LDE
                + 2 * N * 64;           // digest layers (upper bound)
   if (d.with_fri) b += N * 16 + N * 64;  // codeword + FRI layers and trees
