@@ -109,12 +109,52 @@ struct Goldilocks {
   }
   __host__ __device__ __forceinline__ static uint64_t mul(uint64_t a, uint64_t b) {
 #ifdef __CUDA_ARCH__
-    uint64_t lo = a * b, hi = __umul64hi(a, b);
+    // 128-bit product from four 32x32 partial products (eight 32-bit multiplies, one
+    // carry chain), then the reduction with 32-bit adds/subtracts only:
+    //   x = r3*2^96 + r2*2^64 + (r1:r0) = (r1:r0) - r3 + r2*(2^32 - 1)   (mod p)
+    uint32_t r0, r1, r2, r3;
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    asm("mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "addc.u32 %3, %3, 0;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+    uint32_t t0, t1, u0, u1, s0, s1;
+    // t = (r1:r0) - r3, plus p on a borrow (as "- EPS": the raw difference exceeds EPS then)
+    asm("{\n\t.reg .u32 m;\n\t"
+        "sub.cc.u32 %0, %2, %4;\n\t"
+        "subc.cc.u32 %1, %3, 0;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(t0), "=&r"(t1)
+        : "r"(r0), "r"(r1), "r"(r3));
+    // u = r2 * 2^32 - r2 (< 2^64)
+    asm("sub.cc.u32 %0, 0, %2;\n\t"
+        "subc.u32 %1, %2, 0;"
+        : "=&r"(u0), "=&r"(u1)
+        : "r"(r2));
+    // s = t + u, plus EPS on a carry out of 2^64 (2^64 = EPS mod p; no second carry)
+    asm("{\n\t.reg .u32 c;\n\t"
+        "add.cc.u32 %0, %2, %4;\n\t"
+        "addc.cc.u32 %1, %3, %5;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"
+        "add.cc.u32 %0, %0, c;\n\t"
+        "addc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(s0), "=&r"(s1)
+        : "r"(t0), "r"(t1), "r"(u0), "r"(u1));
+    return canon(((uint64_t)s1 << 32) | s0);
 #else
     unsigned __int128 t = (unsigned __int128)a * b;
-    uint64_t lo = (uint64_t)t, hi = (uint64_t)(t >> 64);
+    return reduce128((uint64_t)t, (uint64_t)(t >> 64));
 #endif
-    return reduce128(lo, hi);
   }
   __host__ __device__ __forceinline__ static uint64_t mul_tw(uint64_t x, uint64_t w) { return mul(x, w); }
   static inline uint64_t mul_host(uint64_t a, uint64_t b) { return mul(a, b); }

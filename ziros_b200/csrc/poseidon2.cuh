@@ -47,6 +47,38 @@ __host__ __device__ __forceinline__ typename F::T p2_sbox(typename F::T x) {
   return D::mul(x4, x3);
 }
 
+#ifdef __CUDA_ARCH__
+// One out-of-line copy of the Goldilocks S-box (four 64-bit products): inlined sixteen
+// times per full round the permutation's loop body outgrows the instruction cache and
+// the warps wait on instruction fetch; a call per lane costs a few moves instead.
+static __device__ __noinline__ uint64_t p2_sbox_goldilocks_call(uint64_t x) {
+  return p2_sbox<Goldilocks>(x);
+}
+#endif
+
+#ifdef __CUDA_ARCH__
+// The partial rounds' sixteen diagonal products, out of line for the same reason.
+static __device__ __noinline__ uint64_t p2_mul_goldilocks_call(uint64_t x, uint64_t d) {
+  return Goldilocks::mul(x, d);
+}
+#endif
+
+template <class F>
+__host__ __device__ __forceinline__ typename F::T p2_diag_lane(typename F::T x, typename F::T d) {
+#ifdef __CUDA_ARCH__
+  if constexpr (std::is_same<F, Goldilocks>::value) return p2_mul_goldilocks_call(x, d);
+#endif
+  return P2Dom<F>::mul(x, d);
+}
+
+template <class F>
+__host__ __device__ __forceinline__ typename F::T p2_sbox_lane(typename F::T x) {
+#ifdef __CUDA_ARCH__
+  if constexpr (std::is_same<F, Goldilocks>::value) return p2_sbox_goldilocks_call(x);
+#endif
+  return p2_sbox<F>(x);
+}
+
 template <class F, int W>
 __host__ __device__ __forceinline__ void p2_ext_mds(typename F::T (&s)[W]) {
   using D = P2Dom<F>;
@@ -76,7 +108,7 @@ template <class F, int W>
 __host__ __device__ __forceinline__ void p2_full_round(typename F::T (&s)[W], const typename F::T *rc) {
   using D = P2Dom<F>;
 #pragma unroll
-  for (int i = 0; i < W; i++) s[i] = p2_sbox<F>(D::add(s[i], rc[i]));
+  for (int i = 0; i < W; i++) s[i] = p2_sbox_lane<F>(D::add(s[i], rc[i]));
   p2_ext_mds<F, W>(s);
 }
 
@@ -85,12 +117,12 @@ __host__ __device__ __forceinline__ void p2_partial_round(typename F::T (&s)[W],
                                                  const typename F::T *diag) {
   using D = P2Dom<F>;
   using T = typename F::T;
-  s[0] = p2_sbox<F>(D::add(s[0], rc));
+  s[0] = p2_sbox_lane<F>(D::add(s[0], rc));
   T sum = s[0];
 #pragma unroll
   for (int i = 1; i < W; i++) sum = D::add(sum, s[i]);
 #pragma unroll
-  for (int i = 0; i < W; i++) s[i] = D::add(D::mul(s[i], diag[i]), sum);
+  for (int i = 0; i < W; i++) s[i] = D::add(p2_diag_lane<F>(s[i], diag[i]), sum);
 }
 
 // ------------------------------------------------ BabyBear width 16, specialised
