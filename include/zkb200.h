@@ -241,13 +241,22 @@ ZKB_API int zkb_fri_fold_babybear_ext4(const uint32_t *evals, size_t n_out, cons
  * (x, -x), 8 base elements each (ExtensionMmcs flattening), then folds with beta_r.
  * beta_r = four BabyBear draws (p3 sampler) from SmallRng(challenge_seed); query
  * indices are next_u64() >> (64 - log_n) from SmallRng(query_seed).  Each query opens,
- * per round, the row (index >> r) >> 1 and its sibling path. */
+ * per round, the row (index >> r) >> 1 and its sibling path.
+ * With `transcript` set the challenges come from a DuplexChallenger over the BabyBear
+ * width-16 Poseidon2 of the hasher (see zkb_challenger_*), as p3's prover draws them:
+ * round r observes its root (8 elements) and samples beta_r (4 samples), the final
+ * codeword is observed (element by element, 4 coefficients each), and every query
+ * index is sample_bits(log_n).  The seeds are then unused.  The standalone FRI starts
+ * from a fresh challenger; the commit+FRI job first observes the trace root and samples
+ * alpha.  (p3 observes the final polynomial's coefficients; this transcript observes
+ * the final codeword, which determines them.) */
 typedef struct {
   uint32_t log_n;           /* codeword length 2^log_n extension elements */
   uint32_t log_final;       /* stop at 2^log_final elements */
-  uint64_t challenge_seed;  /* betas */
+  uint64_t challenge_seed;  /* betas (seeded mode) */
   uint32_t num_queries;
-  uint64_t query_seed;
+  uint64_t query_seed;      /* query indices (seeded mode) */
+  uint32_t transcript;      /* 1: challenges from the Fiat-Shamir transcript */
 } zkb_fri_params;
 typedef struct zkb_fri_proof zkb_fri_proof;
 /* Host form: `codeword` holds 2^log_n x 4 u32 (coefficients of each element). */
@@ -267,7 +276,23 @@ ZKB_API int64_t zkb_fri_siblings_per_query(const zkb_fri_proof *proof);
  * sibling paths (num_queries x siblings_per_query u32), round-major within a query. */
 ZKB_API int zkb_fri_query_openings(const zkb_fri_proof *proof, uint64_t *indices_out,
                                    uint32_t *rows_out, uint32_t *siblings_out);
+/* The alpha of the column reduction of a commit+FRI job: the caller's in seeded mode,
+ * the transcript's in transcript mode (4 u32). */
+ZKB_API int zkb_fri_alpha(const zkb_fri_proof *proof, uint32_t *alpha_out);
 ZKB_API void zkb_fri_proof_free(zkb_fri_proof *proof);
+
+/* ------------------------------------------------------------ transcript
+ * p3's DuplexChallenger<F, Poseidon2<16>, 16, 8> (ZirOS: zkf-backends/src/plonky3.rs:66;
+ * native restatement zkf-backends/src/wrapping/duplex_challenger.rs:1-145) over the
+ * width-16 Poseidon2 of `hasher`.  Values are canonical field elements in u64.
+ * sample_bits(b) = the next sample's low b bits (as stark_to_groth16.rs:2229-2255 uses
+ * it).  Host-side; needs no device. */
+typedef struct zkb_challenger zkb_challenger;
+ZKB_API int zkb_challenger_create(const zkb_hasher *hasher, zkb_challenger **out);
+ZKB_API int zkb_challenger_observe(zkb_challenger *c, const uint64_t *values, size_t n);
+ZKB_API int zkb_challenger_sample(zkb_challenger *c, uint64_t *values_out, size_t n);
+ZKB_API int zkb_challenger_sample_bits(zkb_challenger *c, uint32_t bits, uint64_t *out);
+ZKB_API void zkb_challenger_free(zkb_challenger *c);
 
 /* The batched codeword of a PCS opening, without the division by (x - z): for each LDE
  * row i, out[i] = sum_j alpha^j * lde[i][j] in the BabyBear quartic extension — the
@@ -282,7 +307,9 @@ ZKB_API int zkb_combine_columns_babybear_ext4_dev(const uint32_t *d_lde, uint64_
  * of the committed LDE columns into one F_p^4 codeword (zkb_combine_columns_...), then
  * the FRI commit phase and query answers on it (zkb_fri_commit_babybear_ext4;
  * params->log_n is set to log_h + log_blowup).  This is TwoAdicFriPcs commit + open
- * without the (x - z) quotient and the transcript (PCS at zkf-backends/src/plonky3.rs:68).
+ * without the (x - z) quotient (PCS at zkf-backends/src/plonky3.rs:68).  With
+ * params->transcript set, `alpha` is ignored: the transcript observes the trace root
+ * and samples alpha, then drives the FRI challenges (zkb_fri_alpha returns it).
  * Outputs: the trace root (8 u32), the tree (may be NULL) and the FRI proof (may be NULL). */
 ZKB_API int zkb_pcs_commit_fri(const zkb_hasher *hasher, const void *trace, uint32_t log_h,
                                uint32_t width, uint32_t log_blowup, const uint32_t *alpha,

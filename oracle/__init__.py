@@ -299,16 +299,59 @@ def combine_columns_ext4(lde: np.ndarray, alpha) -> np.ndarray:
     return out
 
 
+class DuplexChallenger:
+    """p3 DuplexChallenger<F, Poseidon2<16>, 16, 8>, restated from
+    zkf-backends/src/wrapping/duplex_challenger.rs:1-145 (which mirrors p3-challenger):
+    observe() clears the output buffer and duplexes when 8 inputs are pending; sample()
+    duplexes when input is pending or no output is left and pops the LAST output;
+    duplexing overwrites state[0..len(input)], permutes, outputs state[0..8].
+    sample_bits(b) masks a sample to b bits (stark_to_groth16.rs:2229-2255)."""
+
+    def __init__(self, field: int, p2_seed: int):
+        self.field = field
+        self.rc, self.rf, self.rp = round_constants(field, p2_seed, 16)
+        self.state = np.zeros(16, dtype=dtype_of(field))
+        self.inp, self.out = [], []
+
+    def _duplex(self):
+        for i, v in enumerate(self.inp):
+            self.state[i] = v
+        self.inp = []
+        self.state = permute(self.field, self.state, self.rc, self.rf, self.rp, 16)
+        self.out = [int(x) for x in self.state[:8]]
+
+    def observe(self, values):
+        for v in np.atleast_1d(values):
+            self.out = []
+            self.inp.append(int(v))
+            if len(self.inp) == 8:
+                self._duplex()
+
+    def sample(self, n: int = 1) -> np.ndarray:
+        res = []
+        for _ in range(n):
+            if self.inp or not self.out:
+                self._duplex()
+            res.append(self.out.pop())
+        return np.array(res, dtype=np.uint64)
+
+    def sample_bits(self, bits: int) -> int:
+        return int(self.sample(1)[0]) & ((1 << bits) - 1)
+
+
 def fri_commit_ext4(codeword: np.ndarray, log_final: int, p2_seed: int, challenge_seed: int,
-                    num_queries: int, query_seed: int) -> dict:
-    """FRI commit phase with seeded challenges (p3 commit_phase/answer_query restated):
-    round r commits the codeword as rows of (x, -x) pairs flattened to 8 base elements,
-    then folds with beta_r; queries open row (index >> r) >> 1 of every round."""
+                    num_queries: int, query_seed: int, challenger: DuplexChallenger | None = None) -> dict:
+    """FRI commit phase (p3 commit_phase/answer_query restated): round r commits the
+    codeword as rows of (x, -x) pairs flattened to 8 base elements, then folds with
+    beta_r; queries open row (index >> r) >> 1 of every round.  Challenges: seeded
+    draws, or with `challenger` the transcript (observe root r, sample beta_r; observe
+    the final codeword; query index = sample_bits(log_n))."""
     cw = np.ascontiguousarray(codeword, dtype=np.uint32).reshape(-1, 4)
     log_n = cw.shape[0].bit_length() - 1
     rounds = log_n - log_final
     h = hasher(BABYBEAR, p2_seed)
-    betas = rng_bb(challenge_seed, 4 * rounds).reshape(rounds, 4)
+    betas = rng_bb(challenge_seed, 4 * rounds).reshape(rounds, 4) if challenger is None else \
+        np.zeros((rounds, 4), np.uint32)
     trees, leaves = [], []
     cur = cw
     for r in range(rounds):
@@ -316,8 +359,15 @@ def fri_commit_ext4(codeword: np.ndarray, log_final: int, p2_seed: int, challeng
         layers = mmcs_commit(h, [mat])
         trees.append(layers)
         leaves.append(mat)
+        if challenger is not None:
+            challenger.observe(layers[-1][0])
+            betas[r] = challenger.sample(4).astype(np.uint32)
         cur = fri_fold_ext4(cur, betas[r])
-    idx = (rng_u64(query_seed, num_queries) >> np.uint64(64 - log_n)).astype(np.uint64)
+    if challenger is None:
+        idx = (rng_u64(query_seed, num_queries) >> np.uint64(64 - log_n)).astype(np.uint64)
+    else:
+        challenger.observe(cur.reshape(-1))
+        idx = np.array([challenger.sample_bits(log_n) for _ in range(num_queries)], dtype=np.uint64)
     queries = []
     for q in idx:
         per_round = []

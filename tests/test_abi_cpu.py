@@ -70,3 +70,31 @@ def test_no_device_declines():
     assert "no CUDA device" in N.last_error()
     with pytest.raises(N.ZkbDeclined):
         Z.CudaDft(Z.GOLDILOCKS).dft_batch(np.arange(8, dtype=np.uint64))
+
+
+@pytest.mark.parametrize("field", [0, 1])
+def test_challenger_matches_oracle(oracle, field):
+    """The transcript (DuplexChallenger) runs on the host and needs no device: observe /
+    sample / sample_bits sequences equal the oracle's restatement, including observes
+    that fill the rate exactly, interleaved samples and more samples than the rate."""
+    import numpy as np
+
+    import ziros_b200 as Z
+
+    a, b = oracle.DuplexChallenger(field, 42), Z.Challenger(field, 42)
+    script = [(1, 2, 3, 4, 5), (), tuple(range(8)), (9,) * 9, (100, 200, 300), (), (400, 500), tuple(range(20))]
+    for obs in script:
+        if obs:
+            a.observe(np.array(obs))
+            b.observe(np.array(obs))
+        assert (a.sample(3) == b.sample(3)).all()
+        assert (a.sample(9) == b.sample(9)).all()
+        assert a.sample_bits(22) == b.sample_bits(22)
+
+
+def test_challenger_rejects_non_canonical():
+    import ziros_b200 as Z
+
+    c = Z.Challenger(0, 1)
+    with pytest.raises(Z.ZkbError):
+        c.observe([0x78000001])

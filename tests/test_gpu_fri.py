@@ -123,3 +123,46 @@ def test_pcs_commit_fri_job_matches_oracle(oracle):
     for q in range(10):
         for r in range(pf.rounds):
             assert (pf.query_rows[q, r] == want["queries"][q][r][0]).all()
+
+
+@pytest.mark.parametrize("log_n,log_final,nq", [(6, 2, 10), (13, 3, 30)])
+def test_fri_transcript_matches_oracle(oracle, log_n, log_final, nq):
+    """Transcript mode: beta_r drawn after observing root r, the final codeword observed,
+    query indices from sample_bits(log_n) — every value equal to the oracle's."""
+    cw = rand_field(Z.BABYBEAR, (1 << log_n, 4), 500 + log_n)
+    pf = Z.CudaFriProver(42, log_final, nq, transcript=True).commit(cw)
+    want = oracle.fri_commit_ext4(cw, log_final, 42, 0, nq, 0, challenger=oracle.DuplexChallenger(0, 42))
+    assert (pf.roots == want["roots"]).all() and (pf.betas == want["betas"]).all()
+    assert (pf.final == want["final"]).all() and (pf.query_indices == want["indices"]).all()
+    for q in range(nq):
+        for r in range(pf.rounds):
+            row, proof = want["queries"][q][r]
+            assert (pf.query_rows[q, r] == row).all()
+            assert (pf.siblings(q, r) == np.array(proof).reshape(-1, 8)).all()
+    # the seeds play no part in transcript mode
+    other = Z.CudaFriProver(42, log_final, nq, challenge_seed=99, query_seed=98, transcript=True).commit(cw)
+    assert (other.betas == pf.betas).all() and (other.query_indices == pf.query_indices).all()
+
+
+def test_pcs_commit_fri_transcript_job(oracle):
+    """Commit + FRI with the transcript: alpha is sampled after observing the trace root,
+    then the FRI challenges follow from the same transcript."""
+    trace = rand_field(Z.BABYBEAR, (1 << 10, 24), 41)
+    pcs = Z.CudaTwoAdicPcs(Z.BABYBEAR, 42, 1)
+    root, _, pf = pcs.commit_fri(trace, None, log_final=3, num_queries=12, transcript=True)
+    lde = oracle.coset_lde(Z.BABYBEAR, trace, 1)
+    layers = oracle.mmcs_commit(oracle.hasher(Z.BABYBEAR, 42), [lde])
+    assert (root == layers[-1][0]).all()
+    ch = oracle.DuplexChallenger(0, 42)
+    ch.observe(layers[-1][0])
+    alpha = ch.sample(4).astype(np.uint32)
+    assert (pf.alpha == alpha).all()
+    want = oracle.fri_commit_ext4(oracle.combine_columns_ext4(lde, alpha), 3, 42, 0, 12, 0, challenger=ch)
+    assert (pf.roots == want["roots"]).all() and (pf.betas == want["betas"]).all()
+    assert (pf.final == want["final"]).all() and (pf.query_indices == want["indices"]).all()
+    # the same job through the serving engine
+    eng = Z.CommitEngine(slots=2)
+    r2, pf2, _ = eng.wait(eng.submit(trace, fri={"log_final": 3, "num_queries": 12, "transcript": True}))
+    eng.close()
+    assert (r2 == root).all() and (pf2.alpha == alpha).all() and (pf2.roots == pf.roots).all()
+    assert (pf2.query_indices == pf.query_indices).all()

@@ -8,6 +8,7 @@ from ._native import ZkbDeclined, ZkbError, device_count, load  # noqa: F401
 from .accel import (  # noqa: F401
     BABYBEAR,
     BatchCommit,
+    Challenger,
     CommitEngine,
     GOLDILOCKS,
     CudaDft,

@@ -53,7 +53,7 @@ class Hasher(C.Structure):
 
 class FriParams(C.Structure):
     _fields_ = [("log_n", C.c_uint32), ("log_final", C.c_uint32), ("challenge_seed", C.c_uint64),
-                ("num_queries", C.c_uint32), ("query_seed", C.c_uint64)]
+                ("num_queries", C.c_uint32), ("query_seed", C.c_uint64), ("transcript", C.c_uint32)]
 
 
 class EngineConfig(C.Structure):
@@ -146,6 +146,12 @@ SIGNATURES = {
     "zkb_engine_stats": (_I, [_P, _P]),
     "zkb_engine_destroy": (None, [_P]),
     "zkb_coset_lde_tuned_dev": (_I, [_I, _P, _U32, _U32, _U32, _I, _U32, _U32, _P, _P]),
+    "zkb_fri_alpha": (_I, [_P, _P]),
+    "zkb_challenger_create": (_I, [_P, _P]),
+    "zkb_challenger_observe": (_I, [_P, _P, _SZ]),
+    "zkb_challenger_sample": (_I, [_P, _P, _SZ]),
+    "zkb_challenger_sample_bits": (_I, [_P, _U32, _P]),
+    "zkb_challenger_free": (None, [_P]),
     "zkb_batch_create": (_I, [_P, _P, _SZ, _P, _P]),
     "zkb_batch_trace_ptr": (_I, [_P, _SZ, _P]),
     "zkb_batch_copy_in": (_I, [_P, _SZ, _P, _I, _P]),

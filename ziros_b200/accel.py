@@ -309,10 +309,10 @@ class CudaTwoAdicPcs:
 
     # -- commit + FRI job (BabyBear) ------------------------------------------------
     def _fri_call(self, dev: bool, ptr, stream, h: int, w: int, alpha, log_final: int, num_queries: int,
-                  challenge_seed: int, query_seed: int, want_tree: bool, root):
-        a = np.ascontiguousarray(alpha, dtype=np.uint32)
+                  challenge_seed: int, query_seed: int, want_tree: bool, root, transcript: bool = False):
+        a = np.ascontiguousarray(alpha if alpha is not None else np.zeros(4), dtype=np.uint32)
         log_n = (h.bit_length() - 1) + self.log_blowup
-        prm = N.FriParams(log_n, log_final, challenge_seed, num_queries, query_seed)
+        prm = N.FriParams(log_n, log_final, challenge_seed, num_queries, query_seed, int(transcript))
         root = np.zeros(8, np.uint32) if root is None else root
         th, fh = C.c_void_p(), C.c_void_p()
         args = [C.byref(self.mmcs.hasher), ptr, h.bit_length() - 1, w, self.log_blowup, _ptr(a), C.byref(prm),
@@ -325,24 +325,26 @@ class CudaTwoAdicPcs:
         tree = Tree(th, self.field, [(h << self.log_blowup, w)]) if want_tree else None
         return root, tree, FriProof(fh, prm)
 
-    def commit_fri(self, trace: np.ndarray, alpha, log_final: int, num_queries: int, challenge_seed: int,
-                   query_seed: int, want_tree: bool = True):
+    def commit_fri(self, trace: np.ndarray, alpha, log_final: int, num_queries: int, challenge_seed: int = 0,
+                   query_seed: int = 0, want_tree: bool = True, transcript: bool = False):
         """Commit the trace, reduce its LDE columns with alpha, run the FRI commit phase:
-        returns (root, tree, FriProof)."""
+        returns (root, tree, FriProof).  transcript=True draws alpha, the betas and the
+        query indices from the Fiat-Shamir transcript (alpha and the seeds are ignored)."""
         t = np.ascontiguousarray(trace, dtype=np.uint32)
         return self._fri_call(False, _ptr(t), None, t.shape[0], t.shape[1], alpha, log_final, num_queries,
-                              challenge_seed, query_seed, want_tree, None)
+                              challenge_seed, query_seed, want_tree, None, transcript)
 
     def commit_fri_ptr(self, host_ptr: int, height: int, width: int, alpha, log_final: int, num_queries: int,
-                       challenge_seed: int, query_seed: int, want_tree: bool = False, root=None):
+                       challenge_seed: int = 0, query_seed: int = 0, want_tree: bool = False, root=None,
+                       transcript: bool = False):
         return self._fri_call(False, C.c_void_p(host_ptr), None, height, width, alpha, log_final, num_queries,
-                              challenge_seed, query_seed, want_tree, root)
+                              challenge_seed, query_seed, want_tree, root, transcript)
 
-    def commit_fri_dev(self, trace, alpha, log_final: int, num_queries: int, challenge_seed: int,
-                       query_seed: int, want_tree: bool = False, root=None):
+    def commit_fri_dev(self, trace, alpha, log_final: int, num_queries: int, challenge_seed: int = 0,
+                       query_seed: int = 0, want_tree: bool = False, root=None, transcript: bool = False):
         ptr, stream = _torch_ptr_stream(trace)
         return self._fri_call(True, ptr, stream, trace.shape[0], trace.shape[1], alpha, log_final, num_queries,
-                              challenge_seed, query_seed, want_tree, root)
+                              challenge_seed, query_seed, want_tree, root, transcript)
 
 
 # --------------------------------------------------------------------------- FRI
@@ -402,6 +404,8 @@ class FriProof:
         N.check(lib.zkb_fri_commitments(handle, _ptr(self.roots), _ptr(self.betas)))
         self.final = np.zeros((1 << self.log_final, 4), np.uint32)
         N.check(lib.zkb_fri_final_codeword(handle, _ptr(self.final)))
+        self.alpha = np.zeros(4, np.uint32)  # the column-reduction alpha of a commit+FRI job
+        N.check(lib.zkb_fri_alpha(handle, _ptr(self.alpha)))
         nq = params.num_queries
         spq = lib.zkb_fri_siblings_per_query(handle)
         self.query_indices = np.zeros(nq, np.uint64)
@@ -428,20 +432,23 @@ class FriProof:
 
 
 class CudaFriProver:
-    """FRI commit phase over BabyBear^4 with seeded challenges (p3 prove_fri's commit
-    phase and query answers, as TwoAdicFriPcs runs them)."""
+    """FRI commit phase over BabyBear^4 (p3 prove_fri's commit phase and query answers,
+    as TwoAdicFriPcs runs them), with seeded challenges or, with transcript=True,
+    challenges drawn from a fresh DuplexChallenger."""
 
-    def __init__(self, seed: int, log_final: int, num_queries: int, challenge_seed: int,
-                 query_seed: int):
+    def __init__(self, seed: int, log_final: int, num_queries: int, challenge_seed: int = 0,
+                 query_seed: int = 0, transcript: bool = False):
         N.load()
         self.hasher = N.Hasher(BABYBEAR, 16, seed)
         self.log_final = log_final
         self.num_queries = num_queries
         self.challenge_seed = challenge_seed
         self.query_seed = query_seed
+        self.transcript = transcript
 
     def _params(self, log_n: int) -> "N.FriParams":
-        return N.FriParams(log_n, self.log_final, self.challenge_seed, self.num_queries, self.query_seed)
+        return N.FriParams(log_n, self.log_final, self.challenge_seed, self.num_queries, self.query_seed,
+                           int(self.transcript))
 
     def commit(self, codeword: np.ndarray) -> FriProof:
         cw = np.ascontiguousarray(codeword, dtype=np.uint32).reshape(-1, 4)
@@ -494,8 +501,9 @@ class CommitEngine:
         d.log_h, d.width, d.log_blowup = h.bit_length() - 1, w, log_blowup
         if fri:
             d.with_fri = 1
-            d.alpha[:] = [int(x) for x in fri["alpha"]]
-            d.fri = N.FriParams(0, fri["log_final"], fri["challenge_seed"], fri["num_queries"], fri["query_seed"])
+            d.alpha[:] = [int(x) for x in fri.get("alpha", [0, 0, 0, 0])]
+            d.fri = N.FriParams(0, fri["log_final"], fri.get("challenge_seed", 0), fri["num_queries"],
+                                fri.get("query_seed", 0), int(fri.get("transcript", False)))
         jid = C.c_uint64()
         N.check(N.load().zkb_engine_submit(self._h, C.byref(d), C.byref(jid)))
         self._keep[jid.value] = (t, d)
@@ -515,7 +523,7 @@ class CommitEngine:
         pf = None
         if fh:
             prm = N.FriParams(d.log_h + d.log_blowup, d.fri.log_final, d.fri.challenge_seed, d.fri.num_queries,
-                              d.fri.query_seed)
+                              d.fri.query_seed, d.fri.transcript)
             pf = FriProof(fh, prm)
         return root, pf, {"queue_ms": res.queue_ms, "run_ms": res.run_ms, "latency_ms": res.latency_ms}
 
@@ -531,6 +539,39 @@ class CommitEngine:
 
     def __del__(self):
         self.close()
+
+
+# ------------------------------------------------------------------ transcript
+class Challenger:
+    """p3 DuplexChallenger<F, Poseidon2<16>, 16, 8> (zkb_challenger_*): observe canonical
+    field elements, sample elements or low bits.  Host-side; needs no device."""
+
+    def __init__(self, field: int = BABYBEAR, seed: int = 42):
+        self._h = C.c_void_p()
+        N.check(N.load().zkb_challenger_create(C.byref(N.Hasher(field, 16, seed)), C.byref(self._h)))
+
+    def observe(self, values) -> None:
+        v = np.ascontiguousarray(np.atleast_1d(values), dtype=np.uint64)
+        N.check(N.load().zkb_challenger_observe(self._h, _ptr(v), v.size))
+
+    def sample(self, n: int = 1) -> np.ndarray:
+        out = np.zeros(n, np.uint64)
+        N.check(N.load().zkb_challenger_sample(self._h, _ptr(out), n))
+        return out
+
+    def sample_bits(self, bits: int) -> int:
+        out = C.c_uint64()
+        N.check(N.load().zkb_challenger_sample_bits(self._h, bits, C.byref(out)))
+        return out.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h:
+            try:
+                N.load().zkb_challenger_free(h)
+            except Exception:  # interpreter shutdown
+                pass
 
 
 # ------------------------------------------------------------------ batched commit

@@ -363,9 +363,24 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
     fri_out->owned.push_back(cw);
     fri_out->stream = s;
     ZKB_CHECK_CUDA(cudaGetDevice(&fri_out->device));
-    ZKB_TRY(combine_columns_ext4_dev((const uint32_t *)lde, N, width, alpha, (uint32_t *)cw, s));
+    DuplexChallenger ch;
+    uint32_t a[4];
+    if (fri->transcript) {
+      // the transcript sees the trace commitment before alpha is drawn
+      uint32_t root[8];
+      ZKB_TRY(mmcs_root_to_host(&tree->t, root, s));
+      ZKB_TRY(ch.init(spec));
+      for (uint32_t v : root) ch.observe(v);
+      for (auto &x : a) x = (uint32_t)ch.sample();
+    } else {
+      ZKB_REQUIRE(alpha != nullptr, "null alpha");
+      for (int k = 0; k < 4; k++) a[k] = alpha[k];
+    }
+    for (int k = 0; k < 4; k++) fri_out->alpha[k] = a[k];
+    ZKB_TRY(combine_columns_ext4_dev((const uint32_t *)lde, N, width, a, (uint32_t *)cw, s));
     ZKB_TRY(fri_commit_ext4_dev(spec, (const uint32_t *)cw, log_n, (int)fri->log_final,
-                                fri->challenge_seed, (int)fri->num_queries, fri->query_seed, fri_out, s));
+                                fri->challenge_seed, (int)fri->num_queries, fri->query_seed, fri_out, s,
+                                fri->transcript ? &ch : nullptr));
   }
   return tree_from(tree_out, tree, root_out, s);
 }
@@ -551,8 +566,11 @@ int fri_commit_impl(const zkb_hasher *hasher, const zkb_fri_params *prm, const u
   ZKB_TRY(hasher_spec(hasher, &spec));
   ZKB_REQUIRE(prm != nullptr && out != nullptr, "null arguments");
   auto pf = std::make_unique<zkb_fri_proof>();
+  DuplexChallenger ch;
+  if (prm->transcript) ZKB_TRY(ch.init(spec));
   ZKB_TRY(fri_commit_ext4_dev(spec, d_cw, (int)prm->log_n, (int)prm->log_final, prm->challenge_seed,
-                              (int)prm->num_queries, prm->query_seed, &pf->f, s));
+                              (int)prm->num_queries, prm->query_seed, &pf->f, s,
+                              prm->transcript ? &ch : nullptr));
   *out = pf.release();
   return ZKB_OK;
 }
@@ -609,6 +627,13 @@ int zkb_fri_query_openings(const zkb_fri_proof *p, uint64_t *indices_out, uint32
   if (indices_out) std::memcpy(indices_out, p->f.query_idx.data(), p->f.query_idx.size() * 8);
   if (rows_out) std::memcpy(rows_out, p->f.query_rows.data(), p->f.query_rows.size() * 4);
   if (siblings_out) std::memcpy(siblings_out, p->f.query_sibs.data(), p->f.query_sibs.size() * 4);
+  return ZKB_OK;
+}
+
+int zkb_fri_alpha(const zkb_fri_proof *p, uint32_t *alpha_out) {
+  clear_error();
+  ZKB_REQUIRE(p != nullptr && alpha_out != nullptr, "null arguments");
+  std::memcpy(alpha_out, p->f.alpha.data(), 16);
   return ZKB_OK;
 }
 

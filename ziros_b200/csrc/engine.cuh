@@ -81,13 +81,33 @@ int fri_fold_base_dev(const typename F::T *d_evals, size_t n_out, typename F::T 
 int fri_fold_ext4_dev(const uint32_t *d_evals, size_t n_out, const uint32_t beta[4],
                       uint32_t *d_out, cudaStream_t s);
 
-// FRI commit phase over BabyBear^4 (seeded challenges) and its query openings.
+// ---------------------------------------------------------------- challenger.cu
+// Fiat-Shamir transcript: p3's DuplexChallenger<F, Poseidon2<16>, 16, 8> on the host.
+struct DuplexChallenger {
+  HasherSpec spec;
+  P2Params<BabyBear, 16> p_bb;
+  P2Params<Goldilocks, 16> p_gl;
+  uint64_t state[16] = {0};
+  std::vector<uint64_t> in, out;
+  int init(const HasherSpec &s);
+  void observe(uint64_t v);
+  uint64_t sample();
+  uint64_t sample_bits(int bits);
+
+ private:
+  void permute();
+  void duplexing();
+};
+
+// FRI commit phase over BabyBear^4 and its query openings; the challenges are seeded
+// draws, or come from a DuplexChallenger (transcript mode).
 struct FriProof {
   int device = 0;
   cudaStream_t stream = nullptr;
   int log_n = 0, log_final = 0;
   std::vector<void *> owned;                       // device state: folded codewords, layer trees
   std::vector<std::array<uint32_t, 4>> betas;
+  std::array<uint32_t, 4> alpha{};                 // alpha of the column reduction (commit+FRI jobs)
   std::vector<uint32_t> final_cw;                  // 2^log_final x 4, host
   std::vector<uint32_t> roots;                     // rounds x 8, host
   std::vector<uint64_t> query_idx;
@@ -105,9 +125,12 @@ int pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uin
                 FriProof *fri_out, cudaStream_t s);
 int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
                              const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s);
+// With `ch` set, every round's root is observed before its beta is sampled, the final
+// codeword is observed, and the query indices are sample_bits(log_n) (the seeds are
+// then unused).
 int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int log_n, int log_final,
                         uint64_t challenge_seed, int num_queries, uint64_t query_seed,
-                        FriProof *pf, cudaStream_t s);
+                        FriProof *pf, cudaStream_t s, DuplexChallenger *ch = nullptr);
 
 }  // namespace zkb
 

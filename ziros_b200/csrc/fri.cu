@@ -222,7 +222,7 @@ FriProof::~FriProof() { release_device(); }
 
 int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int log_n, int log_final,
                         uint64_t challenge_seed, int num_queries, uint64_t query_seed,
-                        FriProof *pf, cudaStream_t s) {
+                        FriProof *pf, cudaStream_t s, DuplexChallenger *ch) {
   ZKB_REQUIRE(spec.field == FIELD_BABYBEAR && spec.width == 16,
               "the extension FRI commits with the BabyBear width-16 hasher");
   ZKB_REQUIRE(log_final >= 0 && log_final < log_n && log_n <= 27,
@@ -237,18 +237,22 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
   pf->log_n = log_n;
   pf->log_final = log_final;
   const int rounds = log_n - log_final;
-  // The challenges are seeded draws, so every fold can run before any layer is hashed:
-  // fold all rounds, then hash the trees of all rounds together (one leaf launch, one
-  // launch per tree level across the rounds, one root gather).
-  SmallRng rng(challenge_seed);
-  for (int r = 0; r < rounds; r++) {
-    std::array<uint32_t, 4> beta;
-    for (auto &b : beta) b = sample_babybear(rng);
-    pf->betas.push_back(beta);
-  }
-  SmallRng qr(query_seed);
+  ZKB_REQUIRE(!ch || ch->spec.field == FIELD_BABYBEAR, "the transcript must be over BabyBear");
+  // Seeded challenges: every fold can run before any layer is hashed, so all rounds'
+  // folds run first and the trees of all rounds are hashed together (one leaf launch,
+  // one launch per tree level across the rounds, one root gather).  Transcript
+  // challenges: beta_r depends on round r's root, so the rounds run in order.
   pf->query_idx.resize(num_queries);
-  for (auto &q : pf->query_idx) q = qr.next_u64() >> (64 - log_n);
+  if (!ch) {
+    SmallRng rng(challenge_seed);
+    for (int r = 0; r < rounds; r++) {
+      std::array<uint32_t, 4> beta;
+      for (auto &b : beta) b = sample_babybear(rng);
+      pf->betas.push_back(beta);
+    }
+    SmallRng qr(query_seed);
+    for (auto &q : pf->query_idx) q = qr.next_u64() >> (64 - log_n);
+  }
 
   // ---- one device allocation: folded codewords, digest layers, roots, tables, query answers
   auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
@@ -294,10 +298,6 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
     return r == 0 ? d_codeword : (const uint32_t *)(base + cw_off[r]);
   };
 
-  // ---- folds
-  for (int r = 0; r < rounds; r++)
-    ZKB_TRY(fri_fold_ext4_dev(cw(r), 1ull << (log_n - r - 1), pf->betas[r].data(), (uint32_t *)cw(r + 1), s));
-
   // ---- trees of every round: round r commits 2^(log_n-r-1) rows of 8 (sibling pairs)
   std::vector<const void *> data(rounds);
   std::vector<uint64_t> rows(rounds), widths(rounds, 8);
@@ -307,20 +307,55 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
     rows[r] = 1ull << (log_n - r - 1);
     layers[r] = base + layers_base + lay_off[r] * 32;
   }
-  mt::Tables tab;
-  mt::build_tables(data, rows, widths, layers, layers[0], 8, 4, &tab);
-  mt::LeafJob *d_leaf;
-  mt::CompJob *d_comp;
-  uint64_t *d_root_off;
-  ZKB_TRY(mt::upload_tables(tab, base + tables_off, s, &d_leaf, &d_comp, &d_root_off));
-  ZKB_TRY((mt::launch_trees<BabyBear, 16>(tab, d_leaf, d_comp, d_root_off, layers[0], base + roots_off, p, 128, s,
-                                          "fri_leaf_hash", "fri_compress", "fri_roots")));
+  std::vector<std::vector<uint64_t>> layer_len(rounds);
+  if (!ch) {
+    for (int r = 0; r < rounds; r++)
+      ZKB_TRY(fri_fold_ext4_dev(cw(r), 1ull << (log_n - r - 1), pf->betas[r].data(), (uint32_t *)cw(r + 1), s));
+    mt::Tables tab;
+    mt::build_tables(data, rows, widths, layers, layers[0], 8, 4, &tab);
+    mt::LeafJob *d_leaf;
+    mt::CompJob *d_comp;
+    uint64_t *d_root_off;
+    ZKB_TRY(mt::upload_tables(tab, base + tables_off, s, &d_leaf, &d_comp, &d_root_off));
+    ZKB_TRY((mt::launch_trees<BabyBear, 16>(tab, d_leaf, d_comp, d_root_off, layers[0], base + roots_off, p, 128,
+                                            s, "fri_leaf_hash", "fri_compress", "fri_roots")));
+    layer_len = tab.layer_len;
+  } else {
+    char *tslot = base + tables_off;
+    uint32_t root[8];
+    for (int r = 0; r < rounds; r++) {
+      mt::Tables tab;
+      mt::build_tables({data[r]}, {rows[r]}, {8}, {layers[r]}, layers[r], 8, 4, &tab);
+      mt::LeafJob *d_leaf;
+      mt::CompJob *d_comp;
+      uint64_t *d_root_off;
+      ZKB_TRY(mt::upload_tables(tab, tslot, s, &d_leaf, &d_comp, &d_root_off));
+      tslot += tab.device_bytes();
+      char *d_root = base + roots_off + (size_t)r * 32;
+      ZKB_TRY((mt::launch_trees<BabyBear, 16>(tab, d_leaf, d_comp, d_root_off, layers[r], d_root, p, 128, s,
+                                              "fri_leaf_hash", "fri_compress", "fri_roots")));
+      ZKB_CHECK_CUDA(cudaMemcpyAsync(root, d_root, 32, cudaMemcpyDeviceToHost, s));
+      ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+      for (uint32_t v : root) ch->observe(v);
+      std::array<uint32_t, 4> beta;
+      for (auto &b : beta) b = (uint32_t)ch->sample();
+      pf->betas.push_back(beta);
+      ZKB_TRY(fri_fold_ext4_dev(cw(r), rows[r], beta.data(), (uint32_t *)cw(r + 1), s));
+      layer_len[r] = tab.layer_len[0];
+    }
+  }
 
   // ---- answers to the host: roots, final codeword, query openings
   pf->roots.resize((size_t)rounds * 8);
   ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->roots.data(), base + roots_off, (size_t)rounds * 32, cudaMemcpyDeviceToHost, s));
   pf->final_cw.resize((1ull << log_final) * 4);
   ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->final_cw.data(), cw(rounds), 16ull << log_final, cudaMemcpyDeviceToHost, s));
+  if (ch) {
+    // the final codeword goes into the transcript, then the query indices come out of it
+    ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t v : pf->final_cw) ch->observe(v);
+    for (auto &q : pf->query_idx) q = ch->sample_bits(log_n);
+  }
   if (num_queries > 0) {
     std::vector<FriRoundDesc> descs(rounds);
     for (int r = 0; r < rounds; r++) {
@@ -332,7 +367,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
       uint64_t o = 0;
       for (int l = 0; l < d.depth; l++) {
         d.layer_off[l] = o;
-        o += tab.layer_len[r][l];
+        o += layer_len[r][l];
       }
     }
     ZKB_CHECK_CUDA(cudaMemcpyAsync(base + desc_off, descs.data(), descs.size() * sizeof(FriRoundDesc),
