@@ -200,6 +200,15 @@ ZKB_API int zkb_tree_copy_layer(const zkb_tree *tree, int layer, void *host_out)
 ZKB_API int zkb_mmcs_open_batch(const zkb_tree *tree, uint64_t index, void *rows_out, size_t rows_cap,
                         void *siblings_out, size_t siblings_cap);
 ZKB_API void zkb_tree_free(zkb_tree *tree);
+/* Mmcs::verify_batch (vendor/p3-merkle-tree-gpu/src/mmcs.rs:230-330): checks one opening
+ * against `root` (OUT elements).  heights/widths describe the committed matrices in
+ * commit order; `rows` holds the opened row of every matrix, concatenated in commit
+ * order; `siblings` holds n_siblings = log2(next_pow2(max height)) digests.  ZKB_OK when
+ * the path reproduces the root; ZKB_ERR_INVALID (message: why) otherwise.  Elements are
+ * u32 (BabyBear) or u64 (Goldilocks).  Host-side; needs no device. */
+ZKB_API int zkb_mmcs_verify_batch(const zkb_hasher *hasher, const void *root, const uint64_t *heights,
+                                  const uint64_t *widths, size_t n_mats, uint64_t index, const void *rows,
+                                  const void *siblings, size_t n_siblings);
 
 /* TwoAdicFriPcs::commit for one trace matrix (the PCS type of
  * zkf-backends/src/plonky3.rs:68): coset LDE with shift = field generator, rows

@@ -98,3 +98,36 @@ def test_challenger_rejects_non_canonical():
     c = Z.Challenger(0, 1)
     with pytest.raises(Z.ZkbError):
         c.observe([0x78000001])
+
+
+@pytest.mark.parametrize("field,p2w,shapes", [
+    (0, 16, [(64, 16)]),
+    (0, 16, [(37, 9), (19, 3), (5, 20), (37, 2)]),      # odd heights, injection, equal heights
+    (1, 16, [(128, 8), (32, 5)]),
+    (1, 12, [(16, 7), (8, 1), (2, 3)]),
+])
+def test_verify_batch_accepts_openings_and_rejects_tampering(oracle, field, p2w, shapes):
+    """Mmcs::verify_batch (host-side, no device) against openings of the oracle's trees."""
+    import numpy as np
+
+    import ziros_b200 as Z
+    from conftest import BB_P, GL_P, rand_field
+
+    mats = [rand_field(field, s, 40 + i) for i, s in enumerate(shapes)]
+    layers = oracle.mmcs_commit(oracle.hasher(field, 42, p2w), mats)
+    root = layers[-1][0]
+    mmcs = Z.CudaMerkleTreeMmcs(field, 42, p2w)
+    max_h = max(h for h, _ in shapes)
+    for index in sorted({0, max_h - 1, max_h // 2, 3 % max_h}):
+        rows, proof = oracle.mmcs_open(layers, mats, index)
+        assert mmcs.verify_batch(root, shapes, index, rows, proof)
+        bad_rows = [r.copy() for r in rows]
+        bad_rows[-1][0] = (int(bad_rows[-1][0]) + 1) % (BB_P if field == 0 else GL_P)
+        assert not mmcs.verify_batch(root, shapes, index, bad_rows, proof)
+        if proof:
+            bad_proof = [p.copy() for p in proof]
+            bad_proof[-1][0] ^= 1
+            assert not mmcs.verify_batch(root, shapes, index, rows, bad_proof)
+            assert not mmcs.verify_batch(root, shapes, index ^ 1, rows, proof) or index ^ 1 >= max_h
+    if max_h > 1:  # a proof with the wrong number of siblings is rejected
+        assert not mmcs.verify_batch(root, shapes, 0, oracle.mmcs_open(layers, mats, 0)[0], [])

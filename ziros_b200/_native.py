@@ -147,6 +147,7 @@ SIGNATURES = {
     "zkb_engine_destroy": (None, [_P]),
     "zkb_coset_lde_tuned_dev": (_I, [_I, _P, _U32, _U32, _U32, _I, _U32, _U32, _P, _P]),
     "zkb_fri_alpha": (_I, [_P, _P]),
+    "zkb_mmcs_verify_batch": (_I, [_P, _P, _P, _P, _SZ, _U64, _P, _P, _SZ]),
     "zkb_challenger_create": (_I, [_P, _P]),
     "zkb_challenger_observe": (_I, [_P, _P, _SZ]),
     "zkb_challenger_sample": (_I, [_P, _P, _SZ]),

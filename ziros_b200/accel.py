@@ -246,6 +246,23 @@ class CudaMerkleTreeMmcs:
         t._keepalive = list(mats)
         return root, t
 
+    def verify_batch(self, root, shapes: Sequence[Tuple[int, int]], index: int, rows: Sequence[np.ndarray],
+                     siblings: Sequence[np.ndarray]) -> bool:
+        """Mmcs::verify_batch: True when the opening reproduces the root (host-side)."""
+        dt = dtype_of(self.field)
+        r = np.ascontiguousarray(root, dtype=dt)
+        hs = np.array([s[0] for s in shapes], np.uint64)
+        ws = np.array([s[1] for s in shapes], np.uint64)
+        cat = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=dt).reshape(-1) for x in rows]), dtype=dt)
+        sib = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=dt).reshape(-1) for x in siblings])
+                                   if len(siblings) else np.zeros(0, dt), dtype=dt)
+        rc = N.load().zkb_mmcs_verify_batch(C.byref(self.hasher), _ptr(r), _ptr(hs), _ptr(ws), len(shapes), index,
+                                            _ptr(cat), _ptr(sib), len(siblings))
+        if rc == N.ERR_INVALID:
+            return False
+        N.check(rc)
+        return True
+
     def open_batch(self, index: int, tree: Tree) -> Tuple[List[np.ndarray], List[np.ndarray]]:
         """Mmcs::open_batch -> (rows per matrix, sibling digests)."""
         dt = dtype_of(self.field)

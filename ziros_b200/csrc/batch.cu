@@ -316,7 +316,7 @@ struct zkb_batch {
   }
 
   int tune_lde(TuneCache &cache, bool autotune) {
-    const int kdef = spec.field == FIELD_BABYBEAR ? 11 : 10;
+    const int kdef = spec.field == FIELD_BABYBEAR ? 10 : 7;  // the default plans' largest pass
     std::vector<std::pair<std::string, LdeTune>> done;
     for (size_t i = 0; i < shapes.size(); i++) {
       const std::string key = lde_key(i);

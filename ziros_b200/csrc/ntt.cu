@@ -383,10 +383,14 @@ static int launch_pass(const typename F::T *src, typename F::T *out, const PassG
   return ZKB_ERR_INTERNAL;
 }
 
-// Largest pass: BabyBear up to 64 + 32 values per thread phase, Goldilocks 32 + 32.
+// Largest pass of the default plans (the kernels exist up to 11 bits for BabyBear and 10
+// for Goldilocks, which explicit tuning can still ask for).  Measured on B200 over
+// heights 2^12..2^24: BabyBear is at or near its best with passes of at most 10 bits
+// (an 11-bit pass holds 64 values per thread and runs at lower occupancy), Goldilocks
+// with at most 7 (its 8-byte tiles fill shared memory twice as fast).
 template <class F>
 static constexpr int pass_kmax() {
-  return sizeof(typename F::T) == 4 ? 11 : 10;
+  return sizeof(typename F::T) == 4 ? 10 : 7;
 }
 
 // Runs the passes `ks` (bit counts, top first) starting at index bit hi_start.
