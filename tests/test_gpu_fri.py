@@ -93,7 +93,7 @@ def test_fri_commit_device_resident(oracle):
     assert (pf.roots == want["roots"]).all() and (pf.final == want["final"]).all()
 
 
-@pytest.mark.parametrize("rows,width", [(1, 1), (64, 7), (1 << 12, 256)])
+@pytest.mark.parametrize("rows,width", [(1, 1), (64, 7), (1 << 12, 256), (100, 12), (33, 132), (40, 130)])
 def test_combine_columns_matches_oracle(oracle, rows, width):
     import torch
 

@@ -391,11 +391,13 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
 namespace zkb {
 
 // out[i] = sum_j alpha^j * lde[i][j] over BabyBear^4.  One warp per row: lane l reads
-// columns l, l+32, ... (coalesced), so a warp streams whole rows.  The powers arrive
-// encoded as alpha^j * 2^64 mod p, so each Montgomery product is v * alpha^j * 2^32 and
-// a lane's unreduced 64-bit sum (below p * 2^32 for any width < 2^30) needs one
-// Montgomery reduction to come out as sum v * alpha^j; the 32 lane sums are then added
-// mod p across the warp.
+// columns l, l+32, ... (coalesced; V4 = four consecutive columns per lane with 128-bit
+// loads when the width is a multiple of 4), unrolled so that several loads are in
+// flight per lane.  The powers arrive encoded as alpha^j * 2^64 mod p, so each
+// Montgomery product is v * alpha^j * 2^32 and a lane's unreduced 64-bit sum (below
+// p * 2^32 for any width < 2^30) needs one Montgomery reduction to come out as
+// sum v * alpha^j; the 32 lane sums are then added mod p across the warp.
+template <bool V4>
 __global__ void __launch_bounds__(256)
     combine_columns_kernel(const uint32_t *__restrict__ lde, uint64_t rows, uint32_t width,
                            const uint4 *__restrict__ apow, uint4 *__restrict__ out) {
@@ -405,13 +407,24 @@ __global__ void __launch_bounds__(256)
   for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
     const uint32_t *row = lde + r * width;
     uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-    for (uint32_t j = lane; j < width; j += 32) {
-      const uint32_t v = row[j];
-      const uint4 w = apow[j];
+    auto acc = [&](uint32_t v, uint4 w) {
       a0 += B::mont_lazy(v, w.x);
       a1 += B::mont_lazy(v, w.y);
       a2 += B::mont_lazy(v, w.z);
       a3 += B::mont_lazy(v, w.w);
+    };
+    if constexpr (V4) {
+#pragma unroll 2
+      for (uint32_t j = 4 * lane; j < width; j += 128) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(row + j);
+        acc(v.x, apow[j]);
+        acc(v.y, apow[j + 1]);
+        acc(v.z, apow[j + 2]);
+        acc(v.w, apow[j + 3]);
+      }
+    } else {
+#pragma unroll 4
+      for (uint32_t j = lane; j < width; j += 32) acc(row[j], apow[j]);
     }
     uint32_t c0 = B::mont_reduce(a0), c1 = B::mont_reduce(a1), c2 = B::mont_reduce(a2),
              c3 = B::mont_reduce(a3);
@@ -451,7 +464,11 @@ int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t widt
   DeviceContext *ctx;
   ZKB_TRY(current_context(&ctx));
   ZKB_REQUIRE(width < (1u << 30), "width too large");
-  ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<<<grid_for(rows * 32, 256, (unsigned)ctx->sm_count * 8u), 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
+  const unsigned grid = grid_for(rows * 32, 256, (unsigned)ctx->sm_count * 8u);
+  if (width % 4 == 0 && ((uintptr_t)d_lde & 15) == 0)
+    ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<true><<<grid, 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
+  else
+    ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<false><<<grid, 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
   // the host copy of the powers must outlive the asynchronous upload
   ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
   return ZKB_OK;
