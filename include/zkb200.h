@@ -45,6 +45,7 @@ extern "C" {
 #define ZKB_ERR_UNSUPPORTED (-4)
 #define ZKB_ERR_INTERNAL (-5)
 #define ZKB_ERR_TIMEOUT (-6)
+#define ZKB_ERR_CANCELLED (-7)
 
 #define ZKB_FIELD_BABYBEAR 0
 #define ZKB_FIELD_GOLDILOCKS 1
@@ -60,6 +61,19 @@ ZKB_API const char *zkb_last_error_message(void);
 ZKB_API int zkb_device_count(void);
 /* Select the device used by this thread's subsequent calls. */
 ZKB_API int zkb_set_device(int device);
+
+/* Failure detection, after the reference's watchdog and circuit breaker
+ * (zkf-metal/src/async_dispatch.rs:16-71,162-204; device.rs:649-662): every host wait
+ * on device work has a deadline (env ZKB_WATCHDOG_MS, default 120000; 0 = none).  A
+ * device error or an expired deadline opens a process-wide circuit; while it is open,
+ * every compute entry point declines (ZKB_DECLINED: the caller takes its CPU path).
+ * ZKB_DISABLE=1 declines everything (kill switch, like the reference's ZKF_METAL). */
+ZKB_API int zkb_circuit_open(char *why_out, size_t cap);  /* 1 open (reason copied), 0 closed */
+ZKB_API void zkb_circuit_reset(void);
+/* Host-side fault injection for tests; nothing is injected on the device.  kind 1: the
+ * next `count` device allocations fail as out of memory; kind 2: the next `count` stream
+ * waits report an expired deadline (after the work has finished). */
+ZKB_API int zkb_debug_inject_fault(int kind, int count);
 
 /* Kernel timing.  zkb_profile_start() enables per-launch CUDA events (recorded on
  * the stream each kernel is launched on) and clears earlier records;
@@ -364,6 +378,9 @@ ZKB_API int zkb_engine_submit(zkb_engine *engine, const zkb_job_desc *job, uint6
 /* Blocks until the job is done; fri_out (may be NULL) receives its FRI answers. */
 ZKB_API int zkb_engine_wait(zkb_engine *engine, uint64_t job_id, zkb_job_result *result,
                             zkb_fri_proof **fri_out);
+/* Cancels a job that is still queued (its wait then returns ZKB_ERR_CANCELLED);
+ * ZKB_DECLINED when it has already started. */
+ZKB_API int zkb_engine_cancel(zkb_engine *engine, uint64_t job_id);
 ZKB_API int zkb_engine_stats(zkb_engine *engine, zkb_engine_stats_t *stats);
 /* Finishes the queued jobs, then stops the workers. */
 ZKB_API void zkb_engine_destroy(zkb_engine *engine);

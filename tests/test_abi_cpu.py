@@ -131,3 +131,31 @@ def test_verify_batch_accepts_openings_and_rejects_tampering(oracle, field, p2w,
             assert not mmcs.verify_batch(root, shapes, index ^ 1, rows, proof) or index ^ 1 >= max_h
     if max_h > 1:  # a proof with the wrong number of siblings is rejected
         assert not mmcs.verify_batch(root, shapes, 0, oracle.mmcs_open(layers, mats, 0)[0], [])
+
+
+def test_kill_switch_declines_every_call():
+    """ZKB_DISABLE=1 (the reference's ZKF_METAL kill switch): entry points decline with
+    that reason, before any device is looked for."""
+    import subprocess
+    import sys
+
+    code = ("import numpy as np, ziros_b200 as Z\n"
+            "from ziros_b200 import _native as N\n"
+            "t = np.zeros((16, 4), np.uint32)\n"
+            "try:\n"
+            "    Z.CudaTwoAdicPcs(Z.BABYBEAR, 42, 1).commit(t)\n"
+            "    print('ran')\n"
+            "except N.ZkbDeclined as e:\n"
+            "    print('declined', e)\n")
+    env = dict(os.environ, ZKB_DISABLE="1")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=120,
+                         cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.startswith("declined") and "ZKB_DISABLE" in out.stdout
+
+
+def test_fault_injection_rejects_unknown_kinds():
+    with pytest.raises(Z.ZkbError):
+        N.inject_fault(7, 1)
+    N.inject_fault(1, 0)
+    assert N.circuit_open() == (False, "")

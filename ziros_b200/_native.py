@@ -21,6 +21,7 @@ ERR_OOM = -3
 ERR_UNSUPPORTED = -4
 ERR_INTERNAL = -5
 ERR_TIMEOUT = -6
+ERR_CANCELLED = -7
 
 FIELD_BABYBEAR = 0
 FIELD_GOLDILOCKS = 1
@@ -147,6 +148,10 @@ SIGNATURES = {
     "zkb_engine_destroy": (None, [_P]),
     "zkb_coset_lde_tuned_dev": (_I, [_I, _P, _U32, _U32, _U32, _I, _U32, _U32, _P, _P]),
     "zkb_fri_alpha": (_I, [_P, _P]),
+    "zkb_circuit_open": (_I, [C.c_char_p, _SZ]),
+    "zkb_circuit_reset": (None, []),
+    "zkb_debug_inject_fault": (_I, [_I, _I]),
+    "zkb_engine_cancel": (_I, [_P, _U64]),
     "zkb_mmcs_verify_batch": (_I, [_P, _P, _P, _P, _SZ, _U64, _P, _P, _SZ]),
     "zkb_challenger_create": (_I, [_P, _P]),
     "zkb_challenger_observe": (_I, [_P, _P, _SZ]),
@@ -187,6 +192,21 @@ def load():
             fn.argtypes = args
         _lib = lib
         return lib
+
+
+def circuit_open() -> tuple:
+    """(open, reason) of the library's failure circuit."""
+    buf = C.create_string_buffer(512)
+    return bool(load().zkb_circuit_open(buf, 512)), buf.value.decode(errors="replace")
+
+
+def circuit_reset() -> None:
+    load().zkb_circuit_reset()
+
+
+def inject_fault(kind: int, count: int = 1) -> None:
+    """Host-side fault injection for tests (1: allocations fail, 2: waits time out)."""
+    check(load().zkb_debug_inject_fault(kind, count))
 
 
 def last_error() -> str:

@@ -544,6 +544,15 @@ class CommitEngine:
             pf = FriProof(fh, prm)
         return root, pf, {"queue_ms": res.queue_ms, "run_ms": res.run_ms, "latency_ms": res.latency_ms}
 
+    def cancel(self, job_id: int) -> bool:
+        """Cancels a queued job (its wait then raises with ERR_CANCELLED); False when it
+        has already started."""
+        rc = N.load().zkb_engine_cancel(self._h, job_id)
+        if rc == N.DECLINED:
+            return False
+        N.check(rc)
+        return True
+
     def stats(self) -> dict:
         st = N.EngineStats()
         N.check(N.load().zkb_engine_stats(self._h, C.byref(st)))

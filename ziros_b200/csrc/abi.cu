@@ -21,6 +21,7 @@ namespace {
 
 // Declines (reference fallback semantics) when the process has no usable device.
 int require_device() {
+  ZKB_TRY(library_gate());
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) {
@@ -43,7 +44,7 @@ int to_device(ScratchBuf &buf, const void *host, size_t bytes, cudaStream_t s) {
 
 int to_host(void *host, const void *dev, size_t bytes, cudaStream_t s) {
   if (bytes) ZKB_CHECK_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s));
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  ZKB_TRY(wait_stream(s));
   return ZKB_OK;
 }
 
@@ -96,7 +97,7 @@ int tree_from(zkb_tree **tree_out, std::unique_ptr<zkb_tree> &tree, void *root_o
   if (tree_out)
     *tree_out = tree.release();
   else
-    ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+    ZKB_TRY(wait_stream(s));
   return ZKB_OK;
 }
 
@@ -128,6 +129,24 @@ int zkb_device_count(void) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
   return n;
+}
+
+int zkb_circuit_open(char *why_out, size_t cap) {
+  std::string why;
+  const bool open = circuit_open(&why);
+  if (why_out && cap) {
+    std::snprintf(why_out, cap, "%s", open ? why.c_str() : "");
+  }
+  return open ? 1 : 0;
+}
+
+void zkb_circuit_reset(void) { circuit_reset(); }
+
+int zkb_debug_inject_fault(int kind, int count) {
+  clear_error();
+  const int rc = inject_fault(kind, count);
+  if (rc != ZKB_OK) set_error("unknown fault kind %d or negative count", kind);
+  return rc;
 }
 
 int zkb_set_device(int device) {
@@ -396,7 +415,7 @@ int zkb::pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h
   int rc = pcs_commit_impl(spec, nullptr, h_trace, log_h, width, log_blowup, root_out, nullptr, s,
                            alpha, fri, fri_out);
   if (fri_out) fri_out->release_device();
-  if (rc == ZKB_OK) ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (rc == ZKB_OK) ZKB_TRY(wait_stream(s));
   return rc;
 }
 
@@ -482,7 +501,7 @@ int zkb_tree_copy_layer(const zkb_tree *tree, int layer, void *host_out) {
   ZKB_CHECK_CUDA(cudaSetDevice(t.device));
   ZKB_CHECK_CUDA(cudaMemcpyAsync(host_out, (const char *)t.d_layers + t.layer_off[layer] * D * es,
                                  t.layer_len[layer] * D * es, cudaMemcpyDeviceToHost, t.stream));
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(t.stream));
+  ZKB_TRY(wait_stream(t.stream));
   return ZKB_OK;
 }
 
@@ -528,7 +547,7 @@ int zkb_mmcs_open_batch(const zkb_tree *tree, uint64_t index, void *rows_out, si
                                      cudaMemcpyDeviceToHost, t.stream));
     }
   }
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(t.stream));
+  ZKB_TRY(wait_stream(t.stream));
   return ZKB_OK;
 }
 

@@ -230,7 +230,7 @@ struct zkb_batch {
       cudaGraphExecDestroy(exec);
       exec = nullptr;
     }
-    ZKB_CHECK_CUDA(cudaStreamSynchronize(s_main));
+    ZKB_TRY(wait_stream(s_main));
     if (!d_coef.empty()) cudaFree(d_coef[0]);
     d_coef.clear();
     coef_bytes = 0;
@@ -531,7 +531,7 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   ZKB_CHECK_CUDA(cudaMemsetAsync(b->arena, 0, layers_base, b->s_main));
   ZKB_TRY(mt::upload_tables(b->tables, base + tables_off, b->s_main, &b->d_leaf_jobs, &b->d_comp_jobs,
                             &b->d_root_off));
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(b->s_main));
+  ZKB_TRY(wait_stream(b->s_main));
 
   // ---- streams and events
   for (uint32_t k = 0; k < nb_max; k++) {
@@ -548,7 +548,7 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   b->tune.assign(n, LdeTune{});
   ZKB_TRY(b->assign_branches(1));
   for (size_t i = 0; i < n; i++) ZKB_TRY(b->lde_one(i, b->s_main, nullptr));
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(b->s_main));
+  ZKB_TRY(wait_stream(b->s_main));
   TuneCache cache;
   if (opt.tune_cache) cache.path = opt.tune_cache;
   cache.load();
@@ -598,6 +598,7 @@ int zkb_batch_create(const zkb_hasher *hasher, const zkb_batch_shape *shapes, si
                      const zkb_batch_options *opt, zkb_batch **out) {
   clear_error();
   ZKB_REQUIRE(hasher && shapes && opt && out, "null arguments");
+  ZKB_TRY(library_gate());
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     set_error("no CUDA device available");
@@ -656,6 +657,7 @@ int zkb_batch_copy_in(zkb_batch *b, size_t i, const void *src, int src_on_device
 int zkb_batch_run(zkb_batch *b, void *stream) {
   clear_error();
   ZKB_REQUIRE(b != nullptr, "null batch");
+  ZKB_TRY(library_gate());
   ZKB_CHECK_CUDA(cudaSetDevice(b->device));
   return b->run(resolve_stream(stream));
 }
@@ -667,7 +669,7 @@ int zkb_batch_roots(zkb_batch *b, void *roots_out, void *stream) {
   cudaStream_t s = resolve_stream(stream);
   ZKB_CHECK_CUDA(cudaMemcpyAsync(roots_out, b->d_roots, b->shapes.size() * b->out * b->es,
                                  cudaMemcpyDeviceToHost, s));
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  ZKB_TRY(wait_stream(s));
   return ZKB_OK;
 }
 

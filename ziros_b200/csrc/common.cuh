@@ -68,6 +68,16 @@ inline cudaStream_t resolve_stream(void *s) { return (cudaStream_t)s; }
 
 // Stream-ordered scratch allocation from the device's memory pool.
 int dev_alloc(void **p, size_t bytes, cudaStream_t s);
+// Host wait on a stream with the watchdog deadline (ZKB_WATCHDOG_MS, default 120 s, 0 =
+// none); a device error or an expired deadline opens the circuit.
+int wait_stream(cudaStream_t s);
+bool library_disabled();
+// ZKB_DECLINED (with the reason) when the library is disabled or the circuit is open.
+int library_gate();
+void trip_circuit(const char *why);
+bool circuit_open(std::string *why);
+void circuit_reset();
+int inject_fault(int kind, int count);
 void dev_free(void *p, cudaStream_t s);
 
 // RAII holder for stream-ordered scratch.

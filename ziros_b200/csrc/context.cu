@@ -1,7 +1,12 @@
 // context.cu — per-device context, per-thread streams, last-error, scratch memory.
+#include <atomic>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -166,7 +171,131 @@ int profile_stop(zkb_kernel_stat *out, int cap) {
   return n;
 }
 
+// ------------------------------------------------------- failure detection
+// The reference's watchdog and circuit breaker (zkf-metal/src/async_dispatch.rs:16-71,
+// 162-204; device.rs:649-662): every host wait on device work has a deadline, and a
+// device error or an expired deadline opens a process-wide circuit after which the
+// entry points decline (the caller takes its CPU path) until it is reset.
+namespace {
+std::atomic<bool> g_circuit{false};
+std::mutex g_circuit_mu;
+std::string g_circuit_why;
+std::atomic<int> g_inject_oom{0}, g_inject_timeout{0};
+
+long watchdog_ms() {
+  static const long ms = [] {
+    const char *v = getenv("ZKB_WATCHDOG_MS");
+    return v && *v ? strtol(v, nullptr, 10) : 120000L;
+  }();
+  return ms;
+}
+
+bool take_injected(std::atomic<int> &counter) {
+  int c = counter.load();
+  while (c > 0)
+    if (counter.compare_exchange_weak(c, c - 1)) return true;
+  return false;
+}
+}  // namespace
+
+bool library_disabled() {
+  static const bool off = [] {
+    const char *v = getenv("ZKB_DISABLE");
+    return v && *v && *v != '0';
+  }();
+  return off;
+}
+
+void trip_circuit(const char *why) {
+  std::lock_guard<std::mutex> lk(g_circuit_mu);
+  if (!g_circuit.load()) g_circuit_why = why;
+  g_circuit.store(true);
+}
+
+bool circuit_open(std::string *why) {
+  if (!g_circuit.load()) return false;
+  if (why) {
+    std::lock_guard<std::mutex> lk(g_circuit_mu);
+    *why = g_circuit_why;
+  }
+  return true;
+}
+
+int library_gate() {
+  if (library_disabled()) {
+    set_error("disabled by ZKB_DISABLE");
+    return ZKB_DECLINED;
+  }
+  std::string why;
+  if (circuit_open(&why)) {
+    set_error("circuit open after a device failure (%s); zkb_circuit_reset() closes it", why.c_str());
+    return ZKB_DECLINED;
+  }
+  return ZKB_OK;
+}
+
+void circuit_reset() {
+  std::lock_guard<std::mutex> lk(g_circuit_mu);
+  g_circuit.store(false);
+  g_circuit_why.clear();
+}
+
+int inject_fault(int kind, int count) {
+  if (count < 0) return ZKB_ERR_INVALID;
+  if (kind == 1)
+    g_inject_oom.store(count);
+  else if (kind == 2)
+    g_inject_timeout.store(count);
+  else
+    return ZKB_ERR_INVALID;
+  return ZKB_OK;
+}
+
+int wait_stream(cudaStream_t s) {
+  if (take_injected(g_inject_timeout)) {
+    // simulated expiry: the work is let finish first, so nothing stays in flight
+    cudaStreamSynchronize(s);
+    trip_circuit("watchdog: a stream wait exceeded its deadline (injected)");
+    set_error("watchdog: stream wait exceeded %ld ms (injected)", watchdog_ms());
+    return ZKB_ERR_TIMEOUT;
+  }
+  const long ms = watchdog_ms();
+  cudaError_t e;
+  if (ms <= 0) {
+    e = cudaStreamSynchronize(s);
+  } else {
+    using clk = std::chrono::steady_clock;
+    const auto deadline = clk::now() + std::chrono::milliseconds(ms);
+    int polls = 0;
+    for (;;) {
+      e = cudaStreamQuery(s);
+      if (e != cudaErrorNotReady) break;
+      if (clk::now() > deadline) {
+        trip_circuit("watchdog: a stream wait exceeded its deadline");
+        set_error("watchdog: stream wait exceeded %ld ms", ms);
+        return ZKB_ERR_TIMEOUT;
+      }
+      // spin briefly for short waits, then back off to a few tens of microseconds
+      if (++polls < 64)
+        std::this_thread::yield();
+      else
+        std::this_thread::sleep_for(std::chrono::microseconds(polls < 256 ? 5 : 20));
+    }
+  }
+  if (e != cudaSuccess) {
+    trip_circuit(cudaGetErrorString(e));
+    set_error("device work failed: %s", cudaGetErrorString(e));
+    return ZKB_ERR_CUDA;
+  }
+  return ZKB_OK;
+}
+
 int dev_alloc(void **p, size_t bytes, cudaStream_t s) {
+  if (take_injected(g_inject_oom)) {
+    *p = nullptr;
+    set_error("device allocation of %zu bytes failed: out of memory (injected)", bytes);
+    return ZKB_ERR_OOM;
+  }
   cudaError_t e = cudaMallocAsync(p, bytes, s);
   if (e != cudaSuccess) {
     *p = nullptr;

@@ -335,7 +335,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
       ZKB_TRY((mt::launch_trees<BabyBear, 16>(tab, d_leaf, d_comp, d_root_off, layers[r], d_root, p, 128, s,
                                               "fri_leaf_hash", "fri_compress", "fri_roots")));
       ZKB_CHECK_CUDA(cudaMemcpyAsync(root, d_root, 32, cudaMemcpyDeviceToHost, s));
-      ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+      ZKB_TRY(wait_stream(s));
       for (uint32_t v : root) ch->observe(v);
       std::array<uint32_t, 4> beta;
       for (auto &b : beta) b = (uint32_t)ch->sample();
@@ -352,7 +352,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
   ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->final_cw.data(), cw(rounds), 16ull << log_final, cudaMemcpyDeviceToHost, s));
   if (ch) {
     // the final codeword goes into the transcript, then the query indices come out of it
-    ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+    ZKB_TRY(wait_stream(s));
     for (uint32_t v : pf->final_cw) ch->observe(v);
     for (auto &q : pf->query_idx) q = ch->sample_bits(log_n);
   }
@@ -382,7 +382,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
                                    cudaMemcpyDeviceToHost, s));
   }
   // the host tables above must outlive their (staged) uploads; the answers must be on the host
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  ZKB_TRY(wait_stream(s));
   return ZKB_OK;
 }
 
@@ -470,7 +470,7 @@ int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t widt
   else
     ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<false><<<grid, 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
   // the host copy of the powers must outlive the asynchronous upload
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  ZKB_TRY(wait_stream(s));
   return ZKB_OK;
 }
 

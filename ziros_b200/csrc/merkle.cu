@@ -248,7 +248,7 @@ int mmcs_root_to_host(const DeviceTree *tree, void *root_out, cudaStream_t s) {
   const uint64_t off = tree->layer_off.back() * tree->spec.out;
   ZKB_CHECK_CUDA(cudaMemcpyAsync(root_out, (const char *)tree->d_layers + off * es,
                                  tree->spec.out * es, cudaMemcpyDeviceToHost, s));
-  ZKB_CHECK_CUDA(cudaStreamSynchronize(s));
+  ZKB_TRY(wait_stream(s));
   return ZKB_OK;
 }
 

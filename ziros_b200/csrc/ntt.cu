@@ -97,7 +97,7 @@ int get_twiddles(int log_n, bool inverse, const typename F::T **out, cudaStream_
   T w = two_adic_generator<F>(log_n);
   if (inverse) w = inv_host<F>(w);
   int rc = launch_powers<F>((T *)p, n, w, 1, s);
-  if (rc == ZKB_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = ZKB_ERR_CUDA;
+  if (rc == ZKB_OK) rc = wait_stream(s);
   if (rc != ZKB_OK) {
     cudaFree(p);
     return rc;
@@ -132,7 +132,7 @@ static int get_coset_table(int log_n, int log_b, typename F::T shift, const type
     rc = launch_powers<F>((T *)p + j * n, n, F::mul_host(shift, wj), n_inv, s);
     wj = F::mul_host(wj, w_bn);
   }
-  if (rc == ZKB_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = ZKB_ERR_CUDA;
+  if (rc == ZKB_OK) rc = wait_stream(s);
   if (rc != ZKB_OK) {
     cudaFree(p);
     return rc;

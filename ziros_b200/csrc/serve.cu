@@ -12,6 +12,7 @@
 // The reference has a job-level concurrency scheduler for whole proofs
 // (zkf-metal/src/batch_prover.rs:94-140) and a bounded in-flight command pipeline
 // (zkf-metal/src/pipeline.rs:23-126); this engine is that role for commit jobs.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -142,6 +143,7 @@ int zkb_engine_create(const zkb_engine_config *cfg, zkb_engine **out) {
   clear_error();
   ZKB_REQUIRE(cfg != nullptr && out != nullptr, "null arguments");
   ZKB_REQUIRE(cfg->slots >= 1 && cfg->slots <= 64, "slots must be in [1, 64]");
+  ZKB_TRY(library_gate());
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
     set_error("no CUDA device available");
@@ -172,6 +174,7 @@ int zkb_engine_create(const zkb_engine_config *cfg, zkb_engine **out) {
 int zkb_engine_submit(zkb_engine *e, const zkb_job_desc *desc, uint64_t *job_id) {
   clear_error();
   ZKB_REQUIRE(e != nullptr && desc != nullptr && job_id != nullptr, "null arguments");
+  ZKB_TRY(library_gate());
   ZKB_REQUIRE(desc->trace != nullptr && desc->width > 0 && desc->log_h + desc->log_blowup < 31,
               "bad job shape");
   auto job = std::make_shared<Job>();
@@ -220,6 +223,29 @@ int zkb_engine_wait(zkb_engine *e, uint64_t job_id, zkb_job_result *res, zkb_fri
   if (fri_out) *fri_out = job->fri.release();
   if (job->status != 0) set_error("%s", job->error.c_str());
   return job->status == 0 ? ZKB_OK : job->status;
+}
+
+int zkb_engine_cancel(zkb_engine *e, uint64_t job_id) {
+  clear_error();
+  ZKB_REQUIRE(e != nullptr, "null engine");
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    auto it = e->jobs.find(job_id);
+    ZKB_REQUIRE(it != e->jobs.end(), "unknown job %llu", (unsigned long long)job_id);
+    std::shared_ptr<Job> job = it->second;
+    auto q = std::find(e->queue.begin(), e->queue.end(), job);
+    if (q == e->queue.end()) {
+      set_error("job %llu has already started or finished", (unsigned long long)job_id);
+      return ZKB_DECLINED;
+    }
+    e->queue.erase(q);
+    job->t_start = job->t_done = Clock::now();
+    job->status = ZKB_ERR_CANCELLED;
+    job->error = "cancelled before it started";
+  }
+  e->cv_done.notify_all();
+  e->cv_queue.notify_all();
+  return ZKB_OK;
 }
 
 int zkb_engine_stats(zkb_engine *e, zkb_engine_stats_t *st) {
