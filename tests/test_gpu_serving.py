@@ -85,3 +85,30 @@ def test_rejects_job_larger_than_budget():
     with pytest.raises(Z.ZkbError):
         eng.submit(rand_field(0, (1 << 12, 16), 1))
     eng.close()
+
+
+def test_job_log_lines_and_nvtx_ranges(tmp_path):
+    """ZKB_JOB_LOG writes one JSON line per finished job; ZKB_NVTX=1 wraps launches in
+    NVTX ranges (checked here only for not disturbing the results).  Both are read once
+    per process, so the check runs in a fresh one."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    log = tmp_path / "jobs.jsonl"
+    code = ("import numpy as np, ziros_b200 as Z\n"
+            "rng = np.random.default_rng(1)\n"
+            "e = Z.CommitEngine(slots=2)\n"
+            "ids = [e.submit(rng.integers(0, 0x78000001, size=(1 << h, w), dtype=np.uint32))"
+            " for h, w in ((10, 16), (12, 24))]\n"
+            "roots = [e.wait(i)[0] for i in ids]\n"
+            "e.close()\n"
+            "print(' '.join(str(int(r[0])) for r in roots))\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], env=dict(os.environ, ZKB_JOB_LOG=str(log), ZKB_NVTX="1"),
+                         capture_output=True, text=True, timeout=300, cwd=root)
+    assert out.returncode == 0, out.stderr
+    lines = [json.loads(x) for x in log.read_text().splitlines()]
+    assert sorted((d["log_h"], d["width"]) for d in lines) == [(10, 16), (12, 24)]
+    assert all(d["status"] == 0 and d["latency_ms"] >= d["run_ms"] >= 0 for d in lines)

@@ -108,14 +108,26 @@ int profile_start();
 int profile_stop(zkb_kernel_stat *out, int cap);
 int prof_record(const char *name, cudaStream_t s, int phase, void **token);
 
+// ZKB_NVTX=1: every launch is also an NVTX range named for its kernel, for ncu's
+// --nvtx filters and other NVTX-aware tools (header-only NVTX v3, no library needed).
+bool nvtx_enabled();
+void nvtx_push(const char *name);
+void nvtx_pop();
+
 struct ProfScope {
   void *tok = nullptr;
   cudaStream_t s;
+  bool nvtx = false;
   ProfScope(const char *name, cudaStream_t st) : s(st) {
     if (profiling_enabled()) prof_record(name, s, 0, &tok);
+    if (nvtx_enabled()) {
+      nvtx = true;
+      nvtx_push(name);
+    }
   }
   ~ProfScope() {
     if (tok) prof_record(nullptr, s, 1, &tok);
+    if (nvtx) nvtx_pop();
   }
 };
 

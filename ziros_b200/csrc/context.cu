@@ -9,6 +9,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 
 namespace zkb {
@@ -102,6 +104,16 @@ cudaEvent_t take_event(int dev) {
 }  // namespace
 
 bool profiling_enabled() { return g_prof_on; }
+
+bool nvtx_enabled() {
+  static const bool on = [] {
+    const char *v = getenv("ZKB_NVTX");
+    return v && *v && *v != '0';
+  }();
+  return on;
+}
+void nvtx_push(const char *name) { nvtxRangePushA(name); }
+void nvtx_pop() { nvtxRangePop(); }
 
 int prof_record(const char *name, cudaStream_t s, int phase, void **token) {
   if (phase == 0) {

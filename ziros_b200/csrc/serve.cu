@@ -61,6 +61,25 @@ struct Job {
   std::unique_ptr<zkb_fri_proof> fri;
 };
 
+// ZKB_JOB_LOG=<path>: one JSON line per finished job (shape, status, queue/run/latency ms,
+// cells), appended, for per-job metrics next to the p50/p99 the caller computes.
+void log_job(const Job &j, int rc, Clock::time_point done) {
+  static const char *path = getenv("ZKB_JOB_LOG");
+  if (!path || !*path) return;
+  static std::mutex mu;
+  using ms = std::chrono::duration<double, std::milli>;
+  std::lock_guard<std::mutex> lk(mu);
+  FILE *f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f,
+          "{\"job\": %llu, \"field\": %d, \"log_h\": %u, \"width\": %u, \"log_blowup\": %u, \"fri\": %d, "
+          "\"status\": %d, \"cells\": %llu, \"queue_ms\": %.3f, \"run_ms\": %.3f, \"latency_ms\": %.3f}\n",
+          (unsigned long long)j.id, j.desc.hasher.field, j.desc.log_h, j.desc.width, j.desc.log_blowup,
+          j.desc.with_fri, rc, (unsigned long long)((1ull << j.desc.log_h) * j.desc.width),
+          ms(j.t_start - j.t_submit).count(), ms(done - j.t_start).count(), ms(done - j.t_submit).count());
+  fclose(f);
+}
+
 uint64_t job_bytes(const zkb_job_desc &d) {
   const uint64_t es = d.hasher.field == ZKB_FIELD_BABYBEAR ? 4 : 8;
   const uint64_t n = 1ull << d.log_h, N = n << d.log_blowup;
@@ -121,6 +140,7 @@ struct zkb_engine {
                            job->root, fri ? &fri->f : nullptr, s);
       std::string err = rc == ZKB_OK ? "" : zkb_last_error_message();
       ENGINE_TRACE("end job %llu rc=%d %s\n", (unsigned long long)job->id, rc, err.c_str());
+      log_job(*job, rc, Clock::now());
       {
         std::lock_guard<std::mutex> lk(mu);
         job->t_done = Clock::now();
