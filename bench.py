@@ -47,6 +47,9 @@ WORKLOADS = {
     "babybear_2^14x16_b2": dict(field=0, log_h=14, width=16, log_blowup=1, p2w=16),
     # a smaller case of the default workload for profiler captures (inputs still > L2)
     "babybear_2^18x256_b2": dict(field=0, log_h=18, width=256, log_blowup=1, p2w=16),
+    # the default workload's kernel instances (same NTT plan, same column chunks) on 16 columns,
+    # for profiler captures (LDE 537 MB > L2)
+    "babybear_2^22x16_b2": dict(field=0, log_h=22, width=16, log_blowup=1, p2w=16),
     # a smaller case of the Goldilocks workload for profiler captures (LDE 512 MB > L2)
     "goldilocks_2^18x64_b4": dict(field=1, log_h=18, width=64, log_blowup=2, p2w=16),
     # serving: Poisson arrivals of commit+FRI jobs, log2 rows uniform in [14, 24], widths in [32, 512]

@@ -70,6 +70,18 @@ ZKB_API int zkb_set_device(int device);
  * ZKB_DISABLE=1 declines everything (kill switch, like the reference's ZKF_METAL). */
 ZKB_API int zkb_circuit_open(char *why_out, size_t cap);  /* 1 open (reason copied), 0 closed */
 ZKB_API void zkb_circuit_reset(void);
+/* Fallback thresholds, the reference's ThresholdConfig (zkf-metal/src/tuning.rs:84-111)
+ * with its runtime override (tuning.rs:284-300): the host-pointer entry points decline
+ * (ZKB_DECLINED, "below threshold") for transforms of fewer rows than `ntt`, batches of
+ * fewer permutations than `poseidon2`, trees of fewer leaves than `merkle` and folds of
+ * fewer outputs than `fri`, so the caller runs its CPU path.  Default: no minimum, or
+ * env ZKB_THRESHOLDS="ntt=4096,poseidon2=1000,merkle=2048,fri=1024".  NULL resets to no
+ * minimum.  Device-pointer entry points never decline on size. */
+typedef struct {
+  uint64_t ntt, poseidon2, merkle, fri;
+} zkb_thresholds;
+ZKB_API int zkb_set_thresholds(const zkb_thresholds *thresholds);
+ZKB_API int zkb_get_thresholds(zkb_thresholds *thresholds_out);
 /* Host-side fault injection for tests; nothing is injected on the device.  kind 1: the
  * next `count` device allocations fail as out of memory; kind 2: the next `count` stream
  * waits report an expired deadline (after the work has finished). */

@@ -159,3 +159,19 @@ def test_fault_injection_rejects_unknown_kinds():
         N.inject_fault(7, 1)
     N.inject_fault(1, 0)
     assert N.circuit_open() == (False, "")
+
+
+def test_thresholds_roundtrip_and_environment():
+    N.set_thresholds(ntt=4096, poseidon2=1000, merkle=2048, fri=1024)
+    assert N.get_thresholds() == {"ntt": 4096, "poseidon2": 1000, "merkle": 2048, "fri": 1024}
+    N.set_thresholds()
+    assert N.get_thresholds() == {"ntt": 0, "poseidon2": 0, "merkle": 0, "fri": 0}
+    import subprocess
+    import sys
+
+    code = "from ziros_b200 import _native as N; print(N.get_thresholds())"
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120,
+                         env=dict(os.environ, ZKB_THRESHOLDS="ntt=512,merkle=64"),
+                         cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == str({"ntt": 512, "poseidon2": 0, "merkle": 64, "fri": 0})

@@ -100,3 +100,24 @@ def test_cancel_a_queued_job():
             eng.cancel(ids[0])
     finally:
         eng.close()
+
+
+def test_thresholds_decline_small_host_calls(oracle):
+    """Below a threshold a host-pointer call declines (the caller's CPU path runs); at or
+    above it the call runs on the device as before."""
+    rc, ne, ni = Z.round_constants(Z.BABYBEAR, 42)
+    p2 = Z.CudaPoseidon2()
+    dft = Z.CudaDft(Z.BABYBEAR)
+    try:
+        N.set_thresholds(ntt=1 << 10, poseidon2=1000)
+        assert p2.batch_permute_babybear(np.zeros(16 * 10, np.uint32), rc, ne, ni) is False
+        big = rand_field(Z.BABYBEAR, 16 * 1000, 7)
+        want = oracle.permute(Z.BABYBEAR, big, rc, ne, ni)
+        assert p2.batch_permute_babybear(big, rc, ne, ni) is True and (big == want).all()
+        with pytest.raises(Z.ZkbDeclined) as e:
+            dft.dft_batch(rand_field(Z.BABYBEAR, (1 << 9, 2), 8))
+        assert "below threshold" in str(e.value)
+        m = rand_field(Z.BABYBEAR, (1 << 10, 2), 9)
+        assert (dft.dft_batch(m) == oracle.dft_batch(Z.BABYBEAR, m)).all()
+    finally:
+        N.set_thresholds()

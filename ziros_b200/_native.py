@@ -72,6 +72,10 @@ class JobResult(C.Structure):
                 ("run_ms", C.c_double), ("latency_ms", C.c_double)]
 
 
+class Thresholds(C.Structure):
+    _fields_ = [("ntt", C.c_uint64), ("poseidon2", C.c_uint64), ("merkle", C.c_uint64), ("fri", C.c_uint64)]
+
+
 class BatchShape(C.Structure):
     _fields_ = [("log_h", C.c_uint32), ("width", C.c_uint32)]
 
@@ -148,6 +152,8 @@ SIGNATURES = {
     "zkb_engine_destroy": (None, [_P]),
     "zkb_coset_lde_tuned_dev": (_I, [_I, _P, _U32, _U32, _U32, _I, _U32, _U32, _P, _P]),
     "zkb_fri_alpha": (_I, [_P, _P]),
+    "zkb_set_thresholds": (_I, [_P]),
+    "zkb_get_thresholds": (_I, [_P]),
     "zkb_circuit_open": (_I, [C.c_char_p, _SZ]),
     "zkb_circuit_reset": (None, []),
     "zkb_debug_inject_fault": (_I, [_I, _I]),
@@ -198,6 +204,17 @@ def circuit_open() -> tuple:
     """(open, reason) of the library's failure circuit."""
     buf = C.create_string_buffer(512)
     return bool(load().zkb_circuit_open(buf, 512)), buf.value.decode(errors="replace")
+
+
+def set_thresholds(ntt: int = 0, poseidon2: int = 0, merkle: int = 0, fri: int = 0) -> None:
+    """Minimum sizes below which host-pointer calls decline (all 0: never)."""
+    check(load().zkb_set_thresholds(C.byref(Thresholds(ntt, poseidon2, merkle, fri))))
+
+
+def get_thresholds() -> dict:
+    t = Thresholds()
+    check(load().zkb_get_thresholds(C.byref(t)))
+    return {k: int(getattr(t, k)) for k, _ in Thresholds._fields_}
 
 
 def circuit_reset() -> None:

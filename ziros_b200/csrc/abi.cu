@@ -1,8 +1,11 @@
 // abi.cu — extern "C" entry points declared in include/zkb200.h.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -26,6 +29,51 @@ int require_device() {
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) {
     set_error("no CUDA device available (%s)", e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+    return ZKB_DECLINED;
+  }
+  return ZKB_OK;
+}
+
+// Minimum sizes below which the host-pointer entry points decline so the caller runs its
+// CPU path: the reference's ThresholdConfig (zkf-metal/src/tuning.rs:84-111; ntt = rows,
+// poseidon2 = permutations, merkle = leaves, fri = fold outputs), with a runtime override
+// (tuning.rs:284-300).  Default: no minimum; env ZKB_THRESHOLDS="ntt=4096,poseidon2=1000,..."
+// or zkb_set_thresholds() sets them.
+std::mutex g_thr_mu;
+bool g_thr_init = false;
+zkb_thresholds g_thr{};
+
+zkb_thresholds thresholds() {
+  std::lock_guard<std::mutex> lk(g_thr_mu);
+  if (!g_thr_init) {
+    g_thr_init = true;
+    if (const char *v = getenv("ZKB_THRESHOLDS")) {
+      std::string spec(v);
+      size_t pos = 0;
+      while (pos < spec.size()) {
+        size_t end = spec.find(',', pos);
+        if (end == std::string::npos) end = spec.size();
+        const std::string kv = spec.substr(pos, end - pos);
+        const size_t eq = kv.find('=');
+        if (eq != std::string::npos) {
+          const std::string k = kv.substr(0, eq);
+          const uint64_t x = strtoull(kv.c_str() + eq + 1, nullptr, 10);
+          if (k == "ntt") g_thr.ntt = x;
+          else if (k == "poseidon2") g_thr.poseidon2 = x;
+          else if (k == "merkle") g_thr.merkle = x;
+          else if (k == "fri") g_thr.fri = x;
+        }
+        pos = end + 1;
+      }
+    }
+  }
+  return g_thr;
+}
+
+int below(uint64_t size, uint64_t minimum, const char *what) {
+  if (size < minimum) {
+    set_error("below threshold: %s size %llu < %llu (use the CPU path)", what, (unsigned long long)size,
+              (unsigned long long)minimum);
     return ZKB_DECLINED;
   }
   return ZKB_OK;
@@ -131,6 +179,21 @@ int zkb_device_count(void) {
   return n;
 }
 
+int zkb_set_thresholds(const zkb_thresholds *t) {
+  clear_error();
+  thresholds();  // the environment is read before an override replaces it
+  std::lock_guard<std::mutex> lk(g_thr_mu);
+  g_thr = t ? *t : zkb_thresholds{};
+  return ZKB_OK;
+}
+
+int zkb_get_thresholds(zkb_thresholds *t) {
+  clear_error();
+  ZKB_REQUIRE(t != nullptr, "null output");
+  *t = thresholds();
+  return ZKB_OK;
+}
+
 int zkb_circuit_open(char *why_out, size_t cap) {
   std::string why;
   const bool open = circuit_open(&why);
@@ -203,12 +266,14 @@ int zkb_poseidon2_goldilocks_round_constants(uint64_t seed, uint32_t width, uint
 int zkb_poseidon2_babybear_permute(uint32_t *states, size_t n_elems, const uint32_t *rc, size_t n_rc,
                                    uint32_t n_ext, uint32_t n_int) {
   ZKB_ENTRY();
+  ZKB_TRY(below(n_elems / 16, thresholds().poseidon2, "poseidon2"));
   return permute_host_impl<BabyBear>(states, n_elems, rc, n_rc, n_ext, n_int);
 }
 
 int zkb_poseidon2_goldilocks_permute(uint64_t *states, size_t n_elems, const uint64_t *rc,
                                      size_t n_rc, uint32_t n_ext, uint32_t n_int) {
   ZKB_ENTRY();
+  ZKB_TRY(below(n_elems / 16, thresholds().poseidon2, "poseidon2"));
   return permute_host_impl<Goldilocks>(states, n_elems, rc, n_rc, n_ext, n_int);
 }
 
@@ -240,6 +305,7 @@ int zkb_dft_batch(int field, void *rowmajor, uint32_t log_h, uint32_t width, int
   ZKB_ENTRY();
   ZKB_TRY(check_field(field));
   ZKB_REQUIRE(log_h < 40, "log_h too large");
+  ZKB_TRY(below(1ull << log_h, thresholds().ntt, "ntt"));
   const size_t bytes = ((size_t)width << log_h) * field_elem_bytes(field);
   cudaStream_t s = thread_stream();
   ScratchBuf d;
@@ -289,6 +355,7 @@ int zkb_coset_lde_batch(int field, const void *trace, uint32_t log_h, uint32_t w
   ZKB_ENTRY();
   ZKB_TRY(check_field(field));
   ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
+  ZKB_TRY(below(1ull << log_h, thresholds().ntt, "ntt"));
   const size_t es = field_elem_bytes(field);
   const size_t in_bytes = ((size_t)width << log_h) * es;
   const size_t out_bytes = in_bytes << log_blowup;
@@ -321,6 +388,9 @@ int zkb_mmcs_commit(const zkb_hasher *hasher, const zkb_matrix *mats, size_t n_m
   HasherSpec spec;
   ZKB_TRY(hasher_spec(hasher, &spec));
   ZKB_REQUIRE(mats != nullptr && n_mats > 0, "No matrices given");
+  uint64_t leaves = 0;
+  for (size_t i = 0; i < n_mats; i++) leaves = std::max<uint64_t>(leaves, mats[i].height);
+  ZKB_TRY(below(leaves, thresholds().merkle, "merkle"));
   cudaStream_t s = thread_stream();
   auto tree = std::make_unique<zkb_tree>();
   tree->t.stream = s;
@@ -427,6 +497,7 @@ int zkb_pcs_commit(const zkb_hasher *hasher, const void *trace, uint32_t log_h, 
   HasherSpec spec;
   ZKB_TRY(hasher_spec(hasher, &spec));
   ZKB_REQUIRE(trace != nullptr && width > 0, "empty trace");
+  ZKB_TRY(below(1ull << log_h, thresholds().ntt, "ntt"));
   return pcs_commit_impl(spec, nullptr, trace, log_h, width, log_blowup, root_out, tree_out,
                          thread_stream());
 }
@@ -557,12 +628,14 @@ void zkb_tree_free(zkb_tree *tree) { delete tree; }
 int zkb_fri_fold_goldilocks(const uint64_t *evals, size_t n_evals, uint64_t alpha,
                             const uint64_t *inv_twiddles, uint64_t *out) {
   ZKB_ENTRY();
+  ZKB_TRY(below(n_evals / 2, thresholds().fri, "fri"));
   return fold_host<Goldilocks>(evals, n_evals, alpha, inv_twiddles, out);
 }
 
 int zkb_fri_fold_babybear(const uint32_t *evals, size_t n_evals, uint32_t alpha,
                           const uint32_t *inv_twiddles, uint32_t *out) {
   ZKB_ENTRY();
+  ZKB_TRY(below(n_evals / 2, thresholds().fri, "fri"));
   return fold_host<BabyBear>(evals, n_evals, alpha, inv_twiddles, out);
 }
 
