@@ -355,6 +355,46 @@ ZKB_API int zkb_pcs_commit_fri_dev(const zkb_hasher *hasher, const void *d_trace
                                    const zkb_fri_params *params, void *root_out, zkb_tree **tree_out,
                                    zkb_fri_proof **fri_out, void *stream);
 
+/* ---------------------------------------------------------------- runtime driver
+ * A dispatch driver for the prover runtime's graph nodes (the reference's
+ * GpuDispatchDriver, zkf-runtime/src/metal_driver.rs:55-80, over the ProverOp set of
+ * zkf-runtime/src/graph.rs:51-110): device buffer slots, and nodes that read and write
+ * them, each depending only on earlier nodes, executed in order on one stream.  A node
+ * the device path declines (thresholds, kill switch, open circuit) stops the run with
+ * ZKB_DECLINED and names the node in *fallback_node (the reference's FallbackSignal: the
+ * caller runs that node and the rest on the CPU).  Sizes: rows = 2^log_n. */
+#define ZKB_OP_NTT 1              /* in place on in_slot: rows x width, natural order; inverse */
+#define ZKB_OP_LDE 2              /* in_slot rows x width -> out_slot (rows << log_blowup) x width, bit-reversed rows */
+#define ZKB_OP_POSEIDON_BATCH 3   /* in place on in_slot: count width-16 states; seed */
+#define ZKB_OP_MERKLE 4           /* MMCS of in_slot (rows x width); root -> out_slot (may be -1); seed, hasher_width */
+#define ZKB_OP_FRI_FOLD 5         /* in_slot 2^log_n evaluations -> out_slot 2^(log_n-1); beta; ext4: F_p^4 BabyBear */
+#define ZKB_OP_FRI_QUERY_OPEN 6   /* tree of node tree_node at count u64 indices (in_slot) -> out_slot: per query the
+                                     row then its sibling digests */
+typedef struct {
+  int kind;                /* ZKB_OP_* */
+  int field;               /* ZKB_FIELD_* */
+  uint32_t log_n, width, log_blowup, inverse;
+  uint64_t count;
+  int in_slot, out_slot;
+  uint64_t seed;           /* Poseidon2 seed (PoseidonBatch, Merkle) */
+  uint32_t hasher_width;   /* Merkle: 16 (default when 0) or 12 (Goldilocks) */
+  uint32_t ext4;           /* FriFold over BabyBear^4 */
+  uint32_t beta[4];        /* FriFold challenge (base field: beta[0], or beta[1]:beta[0] for Goldilocks) */
+  int tree_node;           /* FriQueryOpen: the Merkle node whose tree is opened */
+} zkb_rt_node;
+typedef struct zkb_rt zkb_rt;
+ZKB_API int zkb_rt_create(zkb_rt **rt_out);
+ZKB_API int zkb_rt_buffer(zkb_rt *rt, uint64_t bytes, int *slot_out);
+ZKB_API int zkb_rt_write(zkb_rt *rt, int slot, const void *host, uint64_t bytes);
+ZKB_API int zkb_rt_read(zkb_rt *rt, int slot, void *host, uint64_t bytes);
+ZKB_API int zkb_rt_add(zkb_rt *rt, const zkb_rt_node *node, const int *deps, size_t n_deps, int *node_id);
+ZKB_API int zkb_rt_execute(zkb_rt *rt, void *stream, int *fallback_node);
+/* Device time of a node in the last successful run (CUDA events around its launches). */
+ZKB_API int zkb_rt_node_ms(const zkb_rt *rt, int node_id, float *ms);
+/* Tree of an executed Merkle node (borrowed; zkb_mmcs_open_batch works on it). */
+ZKB_API int zkb_rt_tree(const zkb_rt *rt, int node_id, const zkb_tree **tree);
+ZKB_API void zkb_rt_free(zkb_rt *rt);
+
 /* ---------------------------------------------------------------- serving */
 /* Continuous-batching engine for commit jobs (the role of the reference's proof-level
  * scheduler, zkf-metal/src/batch_prover.rs:94-140, and its bounded in-flight pipeline,

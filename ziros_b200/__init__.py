@@ -19,6 +19,7 @@ from .accel import (  # noqa: F401
     CudaMerkleTreeMmcs,
     CudaPoseidon2,
     CudaTwoAdicPcs,
+    ProverRuntime,
     Tree,
     round_constants,
 )

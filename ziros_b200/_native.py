@@ -72,6 +72,13 @@ class JobResult(C.Structure):
                 ("run_ms", C.c_double), ("latency_ms", C.c_double)]
 
 
+class RtNode(C.Structure):
+    _fields_ = [("kind", C.c_int), ("field", C.c_int), ("log_n", C.c_uint32), ("width", C.c_uint32),
+                ("log_blowup", C.c_uint32), ("inverse", C.c_uint32), ("count", C.c_uint64), ("in_slot", C.c_int),
+                ("out_slot", C.c_int), ("seed", C.c_uint64), ("hasher_width", C.c_uint32), ("ext4", C.c_uint32),
+                ("beta", C.c_uint32 * 4), ("tree_node", C.c_int)]
+
+
 class Thresholds(C.Structure):
     _fields_ = [("ntt", C.c_uint64), ("poseidon2", C.c_uint64), ("merkle", C.c_uint64), ("fri", C.c_uint64)]
 
@@ -152,6 +159,15 @@ SIGNATURES = {
     "zkb_engine_destroy": (None, [_P]),
     "zkb_coset_lde_tuned_dev": (_I, [_I, _P, _U32, _U32, _U32, _I, _U32, _U32, _P, _P]),
     "zkb_fri_alpha": (_I, [_P, _P]),
+    "zkb_rt_create": (_I, [_P]),
+    "zkb_rt_buffer": (_I, [_P, _U64, _P]),
+    "zkb_rt_write": (_I, [_P, _I, _P, _U64]),
+    "zkb_rt_read": (_I, [_P, _I, _P, _U64]),
+    "zkb_rt_add": (_I, [_P, _P, _P, _SZ, _P]),
+    "zkb_rt_execute": (_I, [_P, _P, _P]),
+    "zkb_rt_node_ms": (_I, [_P, _I, _P]),
+    "zkb_rt_tree": (_I, [_P, _I, _P]),
+    "zkb_rt_free": (None, [_P]),
     "zkb_set_thresholds": (_I, [_P]),
     "zkb_get_thresholds": (_I, [_P]),
     "zkb_circuit_open": (_I, [C.c_char_p, _SZ]),

@@ -567,6 +567,72 @@ class CommitEngine:
         self.close()
 
 
+# ------------------------------------------------------------------ runtime driver
+class ProverRuntime:
+    """GpuDispatchDriver for the prover runtime's nodes (zkb_rt_*): device buffer slots
+    and Ntt / Lde / PoseidonBatch / Merkle / FriFold / FriQueryOpen nodes that depend on
+    earlier nodes.  execute() returns None, or the id of the node the device path
+    declined (the reference's FallbackSignal: run that node and the rest on the CPU)."""
+
+    NTT, LDE, POSEIDON_BATCH, MERKLE, FRI_FOLD, FRI_QUERY_OPEN = 1, 2, 3, 4, 5, 6
+
+    def __init__(self):
+        self._h = C.c_void_p()
+        N.check(N.load().zkb_rt_create(C.byref(self._h)))
+
+    def buffer(self, nbytes: int) -> int:
+        slot = C.c_int()
+        N.check(N.load().zkb_rt_buffer(self._h, nbytes, C.byref(slot)))
+        return slot.value
+
+    def write(self, slot: int, array: np.ndarray) -> None:
+        a = np.ascontiguousarray(array)
+        N.check(N.load().zkb_rt_write(self._h, slot, _ptr(a), a.nbytes))
+
+    def read(self, slot: int, shape, dtype) -> np.ndarray:
+        out = np.zeros(shape, dtype=dtype)
+        N.check(N.load().zkb_rt_read(self._h, slot, _ptr(out), out.nbytes))
+        return out
+
+    def add(self, kind: int, field: int = BABYBEAR, deps=(), log_n: int = 0, width: int = 0, log_blowup: int = 0,
+            inverse: bool = False, count: int = 0, in_slot: int = -1, out_slot: int = -1, seed: int = 42,
+            hasher_width: int = 16, ext4: bool = False, beta=(0, 0, 0, 0), tree_node: int = -1) -> int:
+        nd = N.RtNode(kind, field, log_n, width, log_blowup, int(inverse), count, in_slot, out_slot, seed,
+                      hasher_width, int(ext4), (C.c_uint32 * 4)(*[int(b) for b in beta]), tree_node)
+        d = np.ascontiguousarray(np.array(deps, dtype=np.int32))
+        nid = C.c_int()
+        N.check(N.load().zkb_rt_add(self._h, C.byref(nd), _ptr(d) if d.size else None, d.size, C.byref(nid)))
+        return nid.value
+
+    def execute(self) -> Optional[int]:
+        fb = C.c_int(-1)
+        rc = N.load().zkb_rt_execute(self._h, None, C.byref(fb))
+        if rc == N.DECLINED:
+            return fb.value
+        N.check(rc)
+        return None
+
+    def node_ms(self, node: int) -> float:
+        ms = C.c_float()
+        N.check(N.load().zkb_rt_node_ms(self._h, node, C.byref(ms)))
+        return ms.value
+
+    def tree(self, node: int, height: int, width: int, field: int = BABYBEAR) -> Tree:
+        """The tree of an executed Merkle node (borrowed from the runtime)."""
+        t = C.c_void_p()
+        N.check(N.load().zkb_rt_tree(self._h, node, C.byref(t)))
+        return Tree(t, field, [(height, width)], owner=self)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h:
+            try:
+                N.load().zkb_rt_free(h)
+            except Exception:  # interpreter shutdown
+                pass
+
+
 # ------------------------------------------------------------------ transcript
 class Challenger:
     """p3 DuplexChallenger<F, Poseidon2<16>, 16, 8> (zkb_challenger_*): observe canonical

@@ -34,51 +34,6 @@ int require_device() {
   return ZKB_OK;
 }
 
-// Minimum sizes below which the host-pointer entry points decline so the caller runs its
-// CPU path: the reference's ThresholdConfig (zkf-metal/src/tuning.rs:84-111; ntt = rows,
-// poseidon2 = permutations, merkle = leaves, fri = fold outputs), with a runtime override
-// (tuning.rs:284-300).  Default: no minimum; env ZKB_THRESHOLDS="ntt=4096,poseidon2=1000,..."
-// or zkb_set_thresholds() sets them.
-std::mutex g_thr_mu;
-bool g_thr_init = false;
-zkb_thresholds g_thr{};
-
-zkb_thresholds thresholds() {
-  std::lock_guard<std::mutex> lk(g_thr_mu);
-  if (!g_thr_init) {
-    g_thr_init = true;
-    if (const char *v = getenv("ZKB_THRESHOLDS")) {
-      std::string spec(v);
-      size_t pos = 0;
-      while (pos < spec.size()) {
-        size_t end = spec.find(',', pos);
-        if (end == std::string::npos) end = spec.size();
-        const std::string kv = spec.substr(pos, end - pos);
-        const size_t eq = kv.find('=');
-        if (eq != std::string::npos) {
-          const std::string k = kv.substr(0, eq);
-          const uint64_t x = strtoull(kv.c_str() + eq + 1, nullptr, 10);
-          if (k == "ntt") g_thr.ntt = x;
-          else if (k == "poseidon2") g_thr.poseidon2 = x;
-          else if (k == "merkle") g_thr.merkle = x;
-          else if (k == "fri") g_thr.fri = x;
-        }
-        pos = end + 1;
-      }
-    }
-  }
-  return g_thr;
-}
-
-int below(uint64_t size, uint64_t minimum, const char *what) {
-  if (size < minimum) {
-    set_error("below threshold: %s size %llu < %llu (use the CPU path)", what, (unsigned long long)size,
-              (unsigned long long)minimum);
-    return ZKB_DECLINED;
-  }
-  return ZKB_OK;
-}
-
 #define ZKB_ENTRY() \
   clear_error();    \
   ZKB_TRY(require_device())
@@ -181,9 +136,7 @@ int zkb_device_count(void) {
 
 int zkb_set_thresholds(const zkb_thresholds *t) {
   clear_error();
-  thresholds();  // the environment is read before an override replaces it
-  std::lock_guard<std::mutex> lk(g_thr_mu);
-  g_thr = t ? *t : zkb_thresholds{};
+  set_thresholds(t ? *t : zkb_thresholds{});
   return ZKB_OK;
 }
 

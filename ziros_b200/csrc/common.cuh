@@ -78,6 +78,10 @@ void trip_circuit(const char *why);
 bool circuit_open(std::string *why);
 void circuit_reset();
 int inject_fault(int kind, int count);
+// Fallback thresholds (zkb_set_thresholds / ZKB_THRESHOLDS) and the check that declines.
+zkb_thresholds thresholds();
+void set_thresholds(const zkb_thresholds &t);
+int below(uint64_t size, uint64_t minimum, const char *what);
 void dev_free(void *p, cudaStream_t s);
 
 // RAII holder for stream-ordered scratch.
