@@ -355,6 +355,19 @@ ZKB_API int zkb_pcs_commit_fri_dev(const zkb_hasher *hasher, const void *d_trace
                                    const zkb_fri_params *params, void *root_out, zkb_tree **tree_out,
                                    zkb_fri_proof **fri_out, void *stream);
 
+/* ------------------------------------------------------------ polynomial ops
+ * PolyOpsAccelerator (zkf-core/src/acceleration.rs:173-194; Metal implementation
+ * zkf-metal/src/poly.rs:37-230), Goldilocks, host pointers, canonical values:
+ *   eval:       out[j] = f(points[j]) (Horner over n_coeffs coefficients, c_0 first);
+ *   coset_eval: out[i] = f(shift * w^i), i < 2^log_n, for 2^log_n coefficients;
+ *   quotient:   out[i] = (evals[i] - f_z) / (w^i - z) on the subgroup of size 2^log_n,
+ *               0 where w^i = z. */
+ZKB_API int zkb_poly_eval_goldilocks(const uint64_t *coeffs, size_t n_coeffs, const uint64_t *points,
+                                     size_t n_points, uint64_t *out);
+ZKB_API int zkb_poly_coset_eval_goldilocks(const uint64_t *coeffs, uint32_t log_n, uint64_t shift, uint64_t *out);
+ZKB_API int zkb_poly_quotient_goldilocks(const uint64_t *evals, uint32_t log_n, uint64_t z, uint64_t f_z,
+                                         uint64_t *out);
+
 /* ---------------------------------------------------------------- runtime driver
  * A dispatch driver for the prover runtime's graph nodes (the reference's
  * GpuDispatchDriver, zkf-runtime/src/metal_driver.rs:55-80, over the ProverOp set of

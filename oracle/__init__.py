@@ -378,3 +378,38 @@ def fri_commit_ext4(codeword: np.ndarray, log_final: int, p2_seed: int, challeng
         queries.append(per_round)
     return {"roots": np.array([t[-1][0] for t in trees]), "betas": betas, "final": cur,
             "indices": idx, "queries": queries}
+
+
+# ------------------------------------------------------------------ polynomial ops
+def poly_eval_gl(coeffs, points) -> np.ndarray:
+    """Horner evaluation (zkf-metal/src/poly.rs:276-283 horner_eval), Python integers."""
+    p = GL_P
+    out = []
+    for x in points:
+        r = 0
+        for c in reversed([int(v) for v in coeffs]):
+            r = (r * int(x) + c) % p
+        out.append(r)
+    return np.array(out, dtype=np.uint64)
+
+
+def poly_coset_eval_gl(coeffs, shift: int, log_n: int) -> np.ndarray:
+    """f(shift * w^i) for i < 2^log_n, w = two_adic_generator(log_n) (poly.rs:337-363)."""
+    p = GL_P
+    w = int(two_adic_generator(1, log_n))
+    pts = [(shift * pow(w, i, p)) % p for i in range(1 << log_n)]
+    return poly_eval_gl(coeffs, pts)
+
+
+def poly_quotient_gl(evals, z: int, f_z: int) -> np.ndarray:
+    """(e_i - f_z) / (w^i - z) on the subgroup, 0 where w^i = z (poly.rs:366-400)."""
+    p = GL_P
+    n = len(evals)
+    w = int(two_adic_generator(1, n.bit_length() - 1))
+    out = []
+    x = 1
+    for e in evals:
+        d = (x - z) % p
+        out.append(0 if d == 0 else ((int(e) - f_z) % p) * pow(d, p - 2, p) % p)
+        x = x * w % p
+    return np.array(out, dtype=np.uint64)

@@ -159,6 +159,9 @@ SIGNATURES = {
     "zkb_engine_destroy": (None, [_P]),
     "zkb_coset_lde_tuned_dev": (_I, [_I, _P, _U32, _U32, _U32, _I, _U32, _U32, _P, _P]),
     "zkb_fri_alpha": (_I, [_P, _P]),
+    "zkb_poly_eval_goldilocks": (_I, [_P, _SZ, _P, _SZ, _P]),
+    "zkb_poly_coset_eval_goldilocks": (_I, [_P, _U32, _U64, _P]),
+    "zkb_poly_quotient_goldilocks": (_I, [_P, _U32, _U64, _U64, _P]),
     "zkb_rt_create": (_I, [_P]),
     "zkb_rt_buffer": (_I, [_P, _U64, _P]),
     "zkb_rt_write": (_I, [_P, _I, _P, _U64]),

@@ -567,6 +567,44 @@ class CommitEngine:
         self.close()
 
 
+# ------------------------------------------------------------------ polynomial ops
+class CudaPolyOps:
+    """PolyOpsAccelerator (MetalPolyOps, zkf-metal/src/poly.rs): Goldilocks batch
+    evaluation, coset evaluation and the opening quotient."""
+
+    @staticmethod
+    def new() -> Optional["CudaPolyOps"]:
+        N.load()
+        return CudaPolyOps() if _have_device() else None
+
+    @staticmethod
+    def _u64(a) -> np.ndarray:
+        return np.ascontiguousarray(a, dtype=np.uint64)
+
+    def batch_eval_goldilocks(self, coeffs, points) -> np.ndarray:
+        c, p = self._u64(coeffs), self._u64(points)
+        out = np.zeros(p.size, np.uint64)
+        N.check(N.load().zkb_poly_eval_goldilocks(_ptr(c), c.size, _ptr(p), p.size, _ptr(out)))
+        return out
+
+    def coset_eval_goldilocks(self, coeffs, shift: int, log_n: int) -> np.ndarray:
+        c = self._u64(coeffs)
+        if c.size != 1 << log_n:
+            raise ValueError("need 2^log_n coefficients")
+        out = np.zeros(c.size, np.uint64)
+        N.check(N.load().zkb_poly_coset_eval_goldilocks(_ptr(c), log_n, shift, _ptr(out)))
+        return out
+
+    def quotient_goldilocks(self, evals, z: int, f_z: int) -> np.ndarray:
+        e = self._u64(evals)
+        n = e.size
+        if n == 0 or n & (n - 1):
+            raise ValueError("need a power-of-two number of evaluations")
+        out = np.zeros(n, np.uint64)
+        N.check(N.load().zkb_poly_quotient_goldilocks(_ptr(e), n.bit_length() - 1, z, f_z, _ptr(out)))
+        return out
+
+
 # ------------------------------------------------------------------ runtime driver
 class ProverRuntime:
     """GpuDispatchDriver for the prover runtime's nodes (zkb_rt_*): device buffer slots
