@@ -14,7 +14,7 @@ jobs commit without the extension FRI phase).
 
 value : whole-job cells/s with the trace resident in HBM (CUDA events on the
         launching stream, max over ranks).
-e2e   : the same metric through the serving engine (zkb_engine_submit/wait, three
+e2e   : the same metric through the serving engine (zkb_engine_submit/wait, four
         slots) with the trace in pinned host memory: every job's H2D copy and the
         D2H read of its root and FRI answers are inside the timed region; one job's
         copy overlaps another's kernels.
@@ -64,7 +64,7 @@ P2_SEED = 42
 TRACE_SEED = 20240607
 FRI = {"log_final": 8, "num_queries": 100, "challenge_seed": 7, "query_seed": 11}
 ALPHA = [123456789, 987654321, 55555, 4242]
-E2E_SLOTS = 3  # engine slots of the e2e leg: a job's H2D copy overlaps two others' kernels
+E2E_SLOTS = 4  # engine slots of the e2e leg: a job's H2D copy overlaps the other jobs' kernels
 METRIC = "trace cells/s committed (LDE+Poseidon2 Merkle+FRI), batched vs plain; p99 ms"
 
 

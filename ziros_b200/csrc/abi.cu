@@ -366,7 +366,7 @@ namespace {
 int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_trace, uint32_t log_h,
                     uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out,
                     cudaStream_t s, const uint32_t *alpha = nullptr, const zkb_fri_params *fri = nullptr,
-                    FriProof *fri_out = nullptr) {
+                    FriProof *fri_out = nullptr, std::mutex *upload_mu = nullptr) {
   ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
   const size_t es = field_elem_bytes(spec.field);
   const uint64_t n = 1ull << log_h, N = n << log_blowup;
@@ -376,7 +376,15 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
   ScratchBuf staged;
   if (h_trace) {
     ZKB_TRY(staged.alloc(n * width * es, s));
-    ZKB_CHECK_CUDA(cudaMemcpyAsync(staged.p, h_trace, n * width * es, cudaMemcpyHostToDevice, s));
+    if (upload_mu) {
+      // one upload at a time: concurrent jobs would split the PCIe link and all start
+      // computing late; serialised, each upload runs under the other jobs' kernels
+      std::lock_guard<std::mutex> lk(*upload_mu);
+      ZKB_CHECK_CUDA(cudaMemcpyAsync(staged.p, h_trace, n * width * es, cudaMemcpyHostToDevice, s));
+      ZKB_TRY(wait_stream(s));
+    } else {
+      ZKB_CHECK_CUDA(cudaMemcpyAsync(staged.p, h_trace, n * width * es, cudaMemcpyHostToDevice, s));
+    }
     d_trace = staged.p;
   }
   void *lde = nullptr;
@@ -434,9 +442,9 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
 // before returning.
 int zkb::pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                      uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
-                     FriProof *fri_out, cudaStream_t s) {
+                     FriProof *fri_out, cudaStream_t s, std::mutex *upload_mu) {
   int rc = pcs_commit_impl(spec, nullptr, h_trace, log_h, width, log_blowup, root_out, nullptr, s,
-                           alpha, fri, fri_out);
+                           alpha, fri, fri_out, upload_mu);
   if (fri_out) fri_out->release_device();
   if (rc == ZKB_OK) ZKB_TRY(wait_stream(s));
   return rc;

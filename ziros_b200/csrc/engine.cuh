@@ -120,9 +120,10 @@ struct FriProof {
 };
 
 // One PCS commit job from host memory (+ FRI when `fri` is set), device state released.
+// upload_mu (may be NULL) serialises the host-to-device copies of concurrent jobs.
 int pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                 uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
-                FriProof *fri_out, cudaStream_t s);
+                FriProof *fri_out, cudaStream_t s, std::mutex *upload_mu = nullptr);
 int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
                              const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s);
 // With `ch` set, every round's root is observed before its beta is sampled, the final

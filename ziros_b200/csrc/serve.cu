@@ -96,6 +96,7 @@ struct zkb_engine {
   int device = 0;
   uint64_t budget = 0, in_use = 0;
   std::mutex mu;
+  std::mutex upload_mu;  // one job's trace crosses PCIe at a time
   std::condition_variable cv_queue, cv_done;
   std::deque<std::shared_ptr<Job>> queue;
   std::map<uint64_t, std::shared_ptr<Job>> jobs;
@@ -137,7 +138,7 @@ struct zkb_engine {
       zkb_fri_params prm = job->desc.fri;
       int rc = pcs_job_run(job->spec, job->desc.trace, job->desc.log_h, job->desc.width,
                            job->desc.log_blowup, job->desc.alpha, job->desc.with_fri ? &prm : nullptr,
-                           job->root, fri ? &fri->f : nullptr, s);
+                           job->root, fri ? &fri->f : nullptr, s, &upload_mu);
       std::string err = rc == ZKB_OK ? "" : zkb_last_error_message();
       ENGINE_TRACE("end job %llu rc=%d %s\n", (unsigned long long)job->id, rc, err.c_str());
       log_job(*job, rc, Clock::now());
