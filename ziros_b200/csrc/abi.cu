@@ -403,16 +403,30 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
                                  h_trace ? staged.as<uint64_t>() : nullptr);
   ZKB_TRY(rc);
   std::vector<TreeMatrix> mats{{lde, N, width}};
-  ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));
+  // With seeded challenges alpha is known before the commitment, so the leaf hash does the
+  // alpha-reduction while it reads each row (one pass over the LDE instead of two); with
+  // the transcript alpha depends on the root and the reduction runs after the tree.
+  void *cw = nullptr;
+  const bool fused_reduction = fri && !fri->transcript && spec.field == FIELD_BABYBEAR && spec.width == 16;
+  ScratchBuf apow;
   if (fri) {
-    // alpha-reduction of the committed columns, then the FRI commit phase on it
     ZKB_REQUIRE(fri_out != nullptr, "internal: FRI job without a proof object");
-    const int log_n = (int)(log_h + log_blowup);
-    void *cw = nullptr;
     ZKB_TRY(dev_alloc(&cw, N * 16, s));
     fri_out->owned.push_back(cw);
     fri_out->stream = s;
     ZKB_CHECK_CUDA(cudaGetDevice(&fri_out->device));
+  }
+  if (fused_reduction) {
+    ZKB_REQUIRE(alpha != nullptr, "null alpha");
+    ZKB_TRY(alpha_powers_dev(alpha, width, &apow, s));
+    const LeafCombine comb{apow.as<uint4>(), (uint4 *)cw};
+    ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s, false, &comb));
+  } else {
+    ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));
+  }
+  if (fri) {
+    // alpha-reduction of the committed columns (unless fused above), then the FRI commit phase
+    const int log_n = (int)(log_h + log_blowup);
     DuplexChallenger ch;
     uint32_t a[4];
     if (fri->transcript) {
@@ -427,7 +441,7 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
       for (int k = 0; k < 4; k++) a[k] = alpha[k];
     }
     for (int k = 0; k < 4; k++) fri_out->alpha[k] = a[k];
-    ZKB_TRY(combine_columns_ext4_dev((const uint32_t *)lde, N, width, a, (uint32_t *)cw, s));
+    if (!fused_reduction) ZKB_TRY(combine_columns_ext4_dev((const uint32_t *)lde, N, width, a, (uint32_t *)cw, s));
     ZKB_TRY(fri_commit_ext4_dev(spec, (const uint32_t *)cw, log_n, (int)fri->log_final,
                                 fri->challenge_seed, (int)fri->num_queries, fri->query_seed, fri_out, s,
                                 fri->transcript ? &ch : nullptr));

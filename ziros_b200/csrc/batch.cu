@@ -557,6 +557,10 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   ZKB_CHECK_CUDA(cudaEventCreate(&t1));
   cudaEventRecord(t0, b->s_main);
   int rc = b->tune_lde(cache, opt.autotune != 0);
+  // one LDE of every trace with its final kernel shapes builds every table those shapes
+  // read (some depend on the pass split), so nothing is built inside a graph capture
+  for (size_t i = 0; i < n && rc == ZKB_OK; i++) rc = b->lde_one(i, b->s_main, &b->tune[i]);
+  if (rc == ZKB_OK) rc = wait_stream(b->s_main);
   if (rc == ZKB_OK) rc = b->tune_leaf_and_branches(cache, opt.autotune != 0, std::min(opt.branches, nb_max));
   cudaEventRecord(t1, b->s_main);
   cudaEventSynchronize(t1);

@@ -57,6 +57,8 @@ struct DeviceContext {
   std::mutex mu;
   std::map<std::tuple<int, int, int>, DeviceTable> twiddles;           // (field, log_n, inverse)
   std::map<std::tuple<int, int, int, uint64_t>, DeviceTable> cosets;   // (field, log_n, log_b, shift)
+  // coset factors and forward twists in the order the fused LDE kernel reads them
+  std::map<std::tuple<int, int, int, uint64_t, int>, DeviceTable> fused;  // (field, log_n, log_b, shift, K)
 };
 
 // Context of the calling thread's current device (initialised on first use).

@@ -69,8 +69,17 @@ struct DeviceTree {
 
 // p3 MerkleTree::new over device matrices; fills layers and the tree description.
 // fri_layer only renames the kernels for the timing hook (fri_leaf_hash / fri_compress).
+// Alpha-reduction done by the leaf hash while it reads the rows (BabyBear width-16, one
+// matrix): out[row] = sum_j alpha^j * row[j] in F_p^4, apow = alpha^j * 2^64 encoded
+// (alpha_powers_dev).
+struct LeafCombine {
+  const uint4 *apow;
+  uint4 *out;
+};
 int mmcs_build_dev(const HasherSpec &h, const std::vector<TreeMatrix> &mats, DeviceTree *tree,
-                   cudaStream_t s, bool fri_layer = false);
+                   cudaStream_t s, bool fri_layer = false, const LeafCombine *comb = nullptr);
+// alpha^j * 2^64 mod p per coefficient, j < width, uploaded (uint4 per column).
+int alpha_powers_dev(const uint32_t alpha[4], uint32_t width, ScratchBuf *out, cudaStream_t s);
 // Copy the root (spec.out elements) to host memory (synchronises the stream).
 int mmcs_root_to_host(const DeviceTree *tree, void *root_out, cudaStream_t s);
 

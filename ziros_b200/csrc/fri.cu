@@ -446,9 +446,7 @@ static void ext4_mul_host(const uint32_t *a, const uint32_t *b, uint32_t *o) {
   for (int k = 0; k < 4; k++) o[k] = (uint32_t)((c[k] + 11 * (k + 4 < 7 ? c[k + 4] : 0)) % BabyBear::P);
 }
 
-int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
-                             const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s) {
-  ZKB_REQUIRE(((uintptr_t)d_out & 15) == 0, "output must be 16-byte aligned");
+int alpha_powers_dev(const uint32_t alpha[4], uint32_t width, ScratchBuf *out, cudaStream_t s) {
   for (int k = 0; k < 4; k++) ZKB_REQUIRE(alpha[k] < BabyBear::P, "alpha is not canonical");
   std::vector<uint32_t> pw((size_t)width * 4);
   uint32_t cur[4] = {1, 0, 0, 0};
@@ -458,9 +456,16 @@ int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t widt
     ext4_mul_host(cur, alpha, nx);
     for (int k = 0; k < 4; k++) cur[k] = nx[k];
   }
+  ZKB_TRY(out->alloc(pw.size() * 4, s));
+  ZKB_CHECK_CUDA(cudaMemcpyAsync(out->p, pw.data(), pw.size() * 4, cudaMemcpyHostToDevice, s));
+  return ZKB_OK;  // a pageable source is staged before the copy call returns
+}
+
+int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
+                             const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s) {
+  ZKB_REQUIRE(((uintptr_t)d_out & 15) == 0, "output must be 16-byte aligned");
   ScratchBuf d_pw;
-  ZKB_TRY(d_pw.alloc(pw.size() * 4, s));
-  ZKB_CHECK_CUDA(cudaMemcpyAsync(d_pw.p, pw.data(), pw.size() * 4, cudaMemcpyHostToDevice, s));
+  ZKB_TRY(alpha_powers_dev(alpha, width, &d_pw, s));
   DeviceContext *ctx;
   ZKB_TRY(current_context(&ctx));
   ZKB_REQUIRE(width < (1u << 30), "width too large");
@@ -469,8 +474,6 @@ int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t widt
     ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<true><<<grid, 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
   else
     ZKB_LAUNCH("combine_columns", s, combine_columns_kernel<false><<<grid, 256, 0, s>>>(d_lde, rows, width, d_pw.as<uint4>(), (uint4 *)d_out));
-  // the host copy of the powers must outlive the asynchronous upload
-  ZKB_TRY(wait_stream(s));
   return ZKB_OK;
 }
 

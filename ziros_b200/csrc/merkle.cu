@@ -12,6 +12,7 @@
 // Unlike the reference's Metal path (zkf-metal/src/merkle.rs:82-90), which falls back
 // to the CPU for rows wider than 8 elements, every width is hashed on the device.
 #include <algorithm>
+#include <type_traits>
 #include <numeric>
 
 #include "common.cuh"
@@ -76,6 +77,43 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// The leaf sponge of one BabyBear matrix with the alpha-reduction of each row fused in:
+// while the row streams through the sponge, out[row] accumulates sum_j alpha^j * row[j]
+// (four Montgomery products per element, 64-bit sums reduced once; the powers are
+// encoded alpha^j * 2^64 so one reduction gives the canonical sum).
+__global__ void __launch_bounds__(128)
+    hash_rows_combine_kernel(const uint32_t *__restrict__ mat, uint64_t width, uint64_t height,
+                             uint32_t *__restrict__ digests, const __grid_constant__ P2Params<BabyBear, 16> p,
+                             const uint4 *__restrict__ apow, uint4 *__restrict__ comb) {
+  using D = Dom<BabyBear>;
+  using B = BabyBear;
+  for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < height;
+       row += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t s[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) s[i] = 0;
+    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    const uint32_t *rp = mat + row * width;
+    for (uint64_t c = 0; c < width; c += 8) {
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if (c + i < width) {
+          const uint32_t v = rp[c + i];
+          const uint4 w = apow[c + i];
+          a0 += B::mont_lazy(v, w.x);
+          a1 += B::mont_lazy(v, w.y);
+          a2 += B::mont_lazy(v, w.z);
+          a3 += B::mont_lazy(v, w.w);
+          s[i] = D::enter(v);
+        }
+      p2_permute<BabyBear, 16>(s, p);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) digests[row * 8 + i] = D::leave(s[i]);
+    comb[row] = make_uint4(B::mont_reduce(a0), B::mont_reduce(a1), B::mont_reduce(a2), B::mont_reduce(a3));
+  }
+}
+
 // next[i] = compress(prev[2i], prev[2i+1]); with `inj` (digests of the rows injected at
 // this layer, inj_h of them) next[i] = compress(that, i < inj_h ? inj[i] : 0).
 template <class F, int W>
@@ -128,7 +166,7 @@ static int log2_ceil(uint64_t x) {
 
 template <class F, int W>
 static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &mats,
-                           DeviceTree *t, cudaStream_t s, bool fri_layer) {
+                           DeviceTree *t, cudaStream_t s, bool fri_layer, const LeafCombine *comb) {
   const char *leaf_name = fri_layer ? "fri_leaf_hash" : "merkle_leaf_hash";
   const char *comp_name = fri_layer ? "fri_compress" : "merkle_compress";
   using T = typename F::T;
@@ -202,7 +240,17 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
   ZKB_TRY(make_list(0, ng, &ml));
   const unsigned thr = 128;
   const unsigned cap = (unsigned)ctx->sm_count * 16u;
-  ZKB_LAUNCH(leaf_name, s, hash_rows_kernel<F, W><<<grid_for(max_h, thr, cap), thr, 0, s>>>(ml, max_h, layers, p));
+  if constexpr (std::is_same<F, BabyBear>::value && W == 16) {
+    if (comb) {
+      ZKB_REQUIRE(nm == 1, "the fused alpha-reduction takes one matrix");
+      ZKB_LAUNCH(leaf_name, s, hash_rows_combine_kernel<<<grid_for(max_h, thr, cap), thr, 0, s>>>((const uint32_t *)ml.ptr[0], ml.width[0], max_h, layers, p, comb->apow, comb->out));
+    } else {
+      ZKB_LAUNCH(leaf_name, s, hash_rows_kernel<F, W><<<grid_for(max_h, thr, cap), thr, 0, s>>>(ml, max_h, layers, p));
+    }
+  } else {
+    ZKB_REQUIRE(comb == nullptr, "the fused alpha-reduction is BabyBear width 16 only");
+    ZKB_LAUNCH(leaf_name, s, hash_rows_kernel<F, W><<<grid_for(max_h, thr, cap), thr, 0, s>>>(ml, max_h, layers, p));
+  }
   ZKB_CHECK_LAUNCH();
   ScratchBuf inj_buf;  // digests of rows injected at one layer (sized for the largest)
 
@@ -234,11 +282,11 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
 }
 
 int mmcs_build_dev(const HasherSpec &h, const std::vector<TreeMatrix> &mats, DeviceTree *tree,
-                   cudaStream_t s, bool fri_layer) {
+                   cudaStream_t s, bool fri_layer, const LeafCombine *comb) {
   ZKB_REQUIRE(!mats.empty(), "No matrices given");
-  if (h.field == FIELD_BABYBEAR && h.width == 16) return build_tree_impl<BabyBear, 16>(h, mats, tree, s, fri_layer);
-  if (h.field == FIELD_GOLDILOCKS && h.width == 16) return build_tree_impl<Goldilocks, 16>(h, mats, tree, s, fri_layer);
-  if (h.field == FIELD_GOLDILOCKS && h.width == 12) return build_tree_impl<Goldilocks, 12>(h, mats, tree, s, fri_layer);
+  if (h.field == FIELD_BABYBEAR && h.width == 16) return build_tree_impl<BabyBear, 16>(h, mats, tree, s, fri_layer, comb);
+  if (h.field == FIELD_GOLDILOCKS && h.width == 16) return build_tree_impl<Goldilocks, 16>(h, mats, tree, s, fri_layer, comb);
+  if (h.field == FIELD_GOLDILOCKS && h.width == 12) return build_tree_impl<Goldilocks, 12>(h, mats, tree, s, fri_layer, comb);
   set_error("unsupported hasher: field %d width %d", h.field, h.width);
   return ZKB_ERR_UNSUPPORTED;
 }

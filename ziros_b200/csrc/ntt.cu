@@ -142,6 +142,54 @@ static int get_coset_table(int log_n, int log_b, typename F::T shift, const type
   return ZKB_OK;
 }
 
+// The fused LDE kernel's tables in the order it reads them (one contiguous run per CTA):
+//   ctab_t[j*n + m_lo*2^K + e] = ctab[j*n + m_lo + e*2^(L-K)]   (coset factors)
+//   ftw_t[m_lo*2^K + e]        = ftw[m_lo * e]                   (forward output twists)
+template <class F>
+__global__ void fused_tables_kernel(const typename F::T *__restrict__ ctab, const typename F::T *__restrict__ ftw,
+                                    int L, int K, int log_b, typename F::T *__restrict__ ctab_t,
+                                    typename F::T *__restrict__ ftw_t) {
+  const uint64_t n = 1ull << L, nc = n << log_b, total = nc + n, mask = (1ull << K) - 1;
+  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (uint64_t)gridDim.x * blockDim.x) {
+    if (idx < nc) {
+      const uint64_t jc = idx >> L, r = idx & (n - 1), m_lo = r >> K, e = r & mask;
+      ctab_t[idx] = ctab[(jc << L) + m_lo + (e << (L - K))];
+    } else {
+      const uint64_t r = idx - nc, m_lo = r >> K, e = r & mask;
+      ftw_t[r] = ftw[m_lo * e];
+    }
+  }
+}
+
+template <class F>
+static int get_fused_tables(int log_n, int log_b, typename F::T shift, int K, const typename F::T *ctab,
+                            const typename F::T *ftw, const typename F::T **ctab_t, const typename F::T **ftw_t,
+                            cudaStream_t s) {
+  using T = typename F::T;
+  DeviceContext *ctx;
+  ZKB_TRY(current_context(&ctx));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto key = std::make_tuple(field_id<F>(), log_n, log_b, (uint64_t)shift, K);
+  const uint64_t n = 1ull << log_n;
+  auto it = ctx->fused.find(key);
+  if (it == ctx->fused.end()) {
+    void *p = nullptr;
+    ZKB_CHECK_CUDA(cudaMalloc(&p, ((n << log_b) + n) * sizeof(T)));
+    T *ct = (T *)p, *ft = ct + (n << log_b);
+    ZKB_LAUNCH("table_fused", s, fused_tables_kernel<F><<<grid_for((n << log_b) + n, 256), 256, 0, s>>>(ctab, ftw, log_n, K, log_b, ct, ft));
+    const int rc = wait_stream(s);
+    if (rc != ZKB_OK) {
+      cudaFree(p);
+      return rc;
+    }
+    it = ctx->fused.emplace(key, DeviceTable{p, ((n << log_b) + n) * sizeof(T)}).first;
+  }
+  *ctab_t = (const T *)it->second.ptr;
+  *ftw_t = *ctab_t + (n << log_b);
+  return ZKB_OK;
+}
+
 // -------------------------------------------------------------- pass kernel
 // One pass handles index bits [lo, lo+K) of every transform: for each fixed value of
 // the other bits (a "group") and each chunk of C columns, one CTA computes the
@@ -490,8 +538,8 @@ template <class F, int LR1, int LR2, int C>
 __global__ void __launch_bounds__(C << LR2)
     lde_fused_kernel(const typename F::T *in, typename F::T *out, const FusedGeom g,
                      const typename F::T *__restrict__ itw, const typename F::T *__restrict__ ftw,
-                     const typename F::T *__restrict__ ctab, const __grid_constant__ SmallTw<F> ist,
-                     const __grid_constant__ SmallTw<F> fst) {
+                     const typename F::T *__restrict__ ctab_t, const typename F::T *__restrict__ ftw_t,
+                     const __grid_constant__ SmallTw<F> ist, const __grid_constant__ SmallTw<F> fst) {
   using T = typename F::T;
   constexpr int R1 = 1 << LR1, R2 = 1 << LR2, K = LR1 + LR2, Q = R1 / R2;
   constexpr int S = PassSmem<LR2, C>::STRIDE;
@@ -515,7 +563,7 @@ __global__ void __launch_bounds__(C << LR2)
     const uint32_t ex = (ii * (__brev(tt) >> (32 - LR1))) << lm;
     itw_in[e] = itw[ex];
     ftw_in[e] = ftw[ex];
-    ftw_out[e] = ftw[m_lo * e];  // < 2^L
+    ftw_out[e] = ftw_t[((size_t)m_lo << K) + e];  // w^(m_lo * e), stored contiguously per m_lo
   }
 
   const size_t colc = (size_t)chunk * C + c;
@@ -558,8 +606,9 @@ __global__ void __launch_bounds__(C << LR2)
   const size_t rs = (size_t)g.width << lm;
   for (int jc = 0; jc < (1 << g.log_b); jc++) {
     __syncthreads();  // previous users of the tile and of cf are done
-    const T *ct = ctab + (uint64_t)jc * g.n + m_lo;
-    for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) cf[e] = ct[(uint64_t)e << lm];
+    // factors of m = m_lo + e * 2^lm, stored contiguously per (coset, m_lo)
+    const T *ct = ctab_t + (uint64_t)jc * g.n + ((size_t)m_lo << K);
+    for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) cf[e] = ct[e];
     __syncthreads();
     {
       T x[R1];
@@ -601,7 +650,7 @@ __global__ void __launch_bounds__(C << LR2)
 template <class F, int LR1, int LR2, int C>
 static int launch_fused_c(const typename F::T *in, typename F::T *out, const FusedGeom &g,
                           const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
-                          cudaStream_t s) {
+                          const typename F::T *ftw_t, cudaStream_t s) {
   using T = typename F::T;
   constexpr unsigned threads = C << LR2;
   const size_t smem = ((size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) + (4u << (LR1 + LR2))) * sizeof(T);
@@ -609,7 +658,7 @@ static int launch_fused_c(const typename F::T *in, typename F::T *out, const Fus
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   const uint64_t ctas = (uint64_t)g.chunks_per_row * g.blocks;
   const SmallTw<F> ist = small_twiddles<F>(true), fst = small_twiddles<F>(false);
-  ZKB_LAUNCH("lde_fused", s, lde_fused_kernel<F, LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(in, out, g, itw, ftw, ctab, ist, fst));
+  ZKB_LAUNCH("lde_fused", s, lde_fused_kernel<F, LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(in, out, g, itw, ftw, ctab, ftw_t, ist, fst));
   return ZKB_OK;
 }
 
@@ -618,11 +667,11 @@ static int launch_fused_c(const typename F::T *in, typename F::T *out, const Fus
 template <class F, int LR1, int LR2>
 static int launch_fused(const typename F::T *in, typename F::T *out, const FusedGeom &g,
                         const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
-                        uint32_t C, cudaStream_t s) {
+                        const typename F::T *ftw_t, uint32_t C, cudaStream_t s) {
   switch (C) {
-    case 8: return launch_fused_c<F, LR1, LR2, 8>(in, out, g, itw, ftw, ctab, s);
-    case 4: return launch_fused_c<F, LR1, LR2, 4>(in, out, g, itw, ftw, ctab, s);
-    case 1: return launch_fused_c<F, LR1, LR2, 1>(in, out, g, itw, ftw, ctab, s);
+    case 8: return launch_fused_c<F, LR1, LR2, 8>(in, out, g, itw, ftw, ctab, ftw_t, s);
+    case 4: return launch_fused_c<F, LR1, LR2, 4>(in, out, g, itw, ftw, ctab, ftw_t, s);
+    case 1: return launch_fused_c<F, LR1, LR2, 1>(in, out, g, itw, ftw, ctab, ftw_t, s);
     default: break;
   }
   set_error("internal: fused LDE column chunk %u", C);
@@ -681,20 +730,20 @@ int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaS
 template <class F>
 static int launch_fused_k(int K, const typename F::T *in, typename F::T *out, const FusedGeom &g,
                           const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
-                          uint32_t C, cudaStream_t s) {
+                          const typename F::T *ftw_t, uint32_t C, cudaStream_t s) {
   switch (K) {
-    case 1: return launch_fused<F, 1, 0>(in, out, g, itw, ftw, ctab, C, s);
-    case 2: return launch_fused<F, 1, 1>(in, out, g, itw, ftw, ctab, C, s);
-    case 3: return launch_fused<F, 2, 1>(in, out, g, itw, ftw, ctab, C, s);
-    case 4: return launch_fused<F, 2, 2>(in, out, g, itw, ftw, ctab, C, s);
-    case 5: return launch_fused<F, 3, 2>(in, out, g, itw, ftw, ctab, C, s);
-    case 6: return launch_fused<F, 3, 3>(in, out, g, itw, ftw, ctab, C, s);
-    case 7: return launch_fused<F, 4, 3>(in, out, g, itw, ftw, ctab, C, s);
-    case 8: return launch_fused<F, 4, 4>(in, out, g, itw, ftw, ctab, C, s);
-    case 9: return launch_fused<F, 5, 4>(in, out, g, itw, ftw, ctab, C, s);
-    case 10: return launch_fused<F, 5, 5>(in, out, g, itw, ftw, ctab, C, s);
+    case 1: return launch_fused<F, 1, 0>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 2: return launch_fused<F, 1, 1>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 3: return launch_fused<F, 2, 1>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 4: return launch_fused<F, 2, 2>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 5: return launch_fused<F, 3, 2>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 6: return launch_fused<F, 3, 3>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 7: return launch_fused<F, 4, 3>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 8: return launch_fused<F, 4, 4>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 9: return launch_fused<F, 5, 4>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 10: return launch_fused<F, 5, 5>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
     case 11:
-      if constexpr (sizeof(typename F::T) == 4) return launch_fused<F, 6, 5>(in, out, g, itw, ftw, ctab, C, s);
+      if constexpr (sizeof(typename F::T) == 4) return launch_fused<F, 6, 5>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
       [[fallthrough]];
     default:
       set_error("internal: fused LDE pass of %d bits", K);
@@ -774,13 +823,15 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
     g.blocks = 1u << (log_h - Kf);
     g.log_b = log_b;
     g.n = n;
+    const T *ctab_t, *ftw_t;
+    ZKB_TRY(get_fused_tables<F>(log_h, log_b, shift, Kf, ctab, ftw, &ctab_t, &ftw_t, s));
     for (const ColSeg &sg : col_segments(width, tn.c_fused ? tn.c_fused : 8)) {
       g.chunks_per_row = sg.cols / sg.C;
       if ((uint64_t)g.chunks_per_row * g.blocks >= (1ull << 31)) {
         set_error("LDE launch too large");
         return ZKB_ERR_UNSUPPORTED;
       }
-      ZKB_TRY(launch_fused_k<F>(Kf, src + sg.col0, d_out + sg.col0, g, itw, ftw, ctab, sg.C, s));
+      ZKB_TRY(launch_fused_k<F>(Kf, src + sg.col0, d_out + sg.col0, g, itw, ftw, ctab_t, ftw_t, sg.C, s));
     }
     std::vector<int> tail(ks.rbegin() + 1, ks.rend());
     if (!tail.empty())
