@@ -657,6 +657,89 @@ def run_batch(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     return 0
 
 
+def run_sharded(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
+    """One commitment of the workload's trace split over the ranks (ziros_b200.sharded):
+    each rank extends its columns, one all-to-all moves row blocks, each rank hashes its
+    rows, the subtree roots are gathered; with FRI the reduced codeword is gathered and
+    folded on every rank.  The trace is fixed as ranks are added (strong scaling)."""
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from ziros_b200 import _native as N
+    from ziros_b200 import sharded as S
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    N.check(N.load().zkb_set_device(local_rank))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    field, lb = wl["field"], wl["log_blowup"]
+    n, w = 1 << wl["log_h"], wl["width"]
+    c0, c1 = S.column_ranges(w, world)[rank]
+    cols = fill_uniform(torch, field, (n, c1 - c0), TRACE_SEED + rank, dev)
+    ops = S.CudaShardOps(field, P2_SEED, lb, wl["p2w"], dev)
+    fri = S.FriArgs(FRI["log_final"], FRI["num_queries"], ALPHA, FRI["challenge_seed"], FRI["query_seed"]) \
+        if field == 0 else None
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(args.warmup, 1)):
+        ref = S.commit_sharded(cols, w, ops, fri=fri).root
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    barrier()
+    if sampler:
+        sampler.start()
+        time.sleep(0.4)
+    N.profile_start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        res = S.commit_sharded(cols, w, ops, fri=fri)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    kstats = N.profile_stop()
+    clocks = sampler.stop() if sampler else None
+    t = ev0.elapsed_time(ev1) / 1e3
+    if world > 1:
+        tt = torch.tensor([t], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    assert np.array_equal(res.root, ref), "root changed between steps"
+    del res
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    esize = 4 if field == 0 else 8
+    line = {
+        "metric": METRIC, "value": n * w * args.steps / t, "unit": "cells/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32" if field == 0 else "u64",
+        "data": "synthetic (seeded uniform field elements; each rank generates its own columns)",
+        "config": {"workload": args.workload, "log_rows": wl["log_h"], "width": w, "log_blowup": lb,
+                   "poseidon2_width": wl["p2w"],
+                   "parallelism": f"one commitment over {world} ranks: column-sharded LDE, all-to-all of "
+                                  f"row blocks, row-sharded hashing",
+                   "l2": "inputs larger than L2 (trace %.1f GB)" % (n * w * esize / 1e9)},
+        "e2e": None,
+        "note": "device-resident only: the trace starts in each rank's HBM",
+        "gpu_launches": sum(v[0] for v in kstats.values()),
+        "kernels": {k: {"launches": v[0], "ms_total": round(v[1], 3)}
+                    for k, v in sorted(kstats.items(), key=lambda kv: -kv[1][1])},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def serving_jobs(wl: dict, n: int, seed: int) -> list:
     import numpy as np
 
@@ -789,6 +872,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
+    ap.add_argument("--sharded", action="store_true",
+                    help="one commitment split over the ranks (strong scaling) instead of replicas")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", "0"))
@@ -800,6 +885,8 @@ def main() -> int:
         return run_batch(args, wl, rank, world, local_rank)
     if wl.get("kind") == "serving":
         return run_serving(args, wl, rank, world, local_rank)
+    if args.sharded:
+        return run_sharded(args, wl, rank, world, local_rank)
     return run_ours(args, wl, rank, world, local_rank)
 
 

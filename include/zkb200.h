@@ -236,6 +236,13 @@ ZKB_API int zkb_mmcs_verify_batch(const zkb_hasher *hasher, const void *root, co
                                   const uint64_t *widths, size_t n_mats, uint64_t index, const void *rows,
                                   const void *siblings, size_t n_siblings);
 
+/* TruncatedPermutation<Perm, 2, OUT, W> (zkf-backends/src/plonky3.rs:56) of n digest pairs:
+ * out[i] = compress(left[i], right[i]), OUT elements per digest (8 for width 16, 4 for
+ * width 12), u32 (BabyBear) or u64 (Goldilocks).  It finishes the top levels of a tree
+ * whose subtrees were built apart (one per device).  Host-side; needs no device. */
+ZKB_API int zkb_mmcs_compress(const zkb_hasher *hasher, const void *left, const void *right, size_t n,
+                              void *out);
+
 /* TwoAdicFriPcs::commit for one trace matrix (the PCS type of
  * zkf-backends/src/plonky3.rs:68): coset LDE with shift = field generator, rows
  * bit-reversed, MMCS commit of the result — coset_lde_batch + bit_reverse_rows +
@@ -328,6 +335,18 @@ ZKB_API int zkb_challenger_observe(zkb_challenger *c, const uint64_t *values, si
 ZKB_API int zkb_challenger_sample(zkb_challenger *c, uint64_t *values_out, size_t n);
 ZKB_API int zkb_challenger_sample_bits(zkb_challenger *c, uint32_t bits, uint64_t *out);
 ZKB_API void zkb_challenger_free(zkb_challenger *c);
+/* The FRI commit phase driven by a caller's transcript: like zkb_fri_commit_babybear_ext4_dev
+ * in transcript mode (params->transcript and the seeds are ignored), but the challenger is
+ * the caller's, in whatever state earlier observations left it, and it is advanced by the
+ * call — as p3's prover threads one challenger from the trace commitment through alpha into
+ * FRI (p3-fri 0.4.2 prove, over zkf-backends/src/plonky3.rs:66).  Used when the trace root is
+ * known before the reduced codeword exists on this device (a commitment built over several
+ * devices). */
+ZKB_API int zkb_fri_commit_babybear_ext4_challenger_dev(const zkb_hasher *hasher,
+                                                        const zkb_fri_params *params,
+                                                        const uint32_t *d_codeword,
+                                                        zkb_challenger *challenger,
+                                                        zkb_fri_proof **proof_out, void *stream);
 
 /* The batched codeword of a PCS opening, without the division by (x - z): for each LDE
  * row i, out[i] = sum_j alpha^j * lde[i][j] in the BabyBear quartic extension — the

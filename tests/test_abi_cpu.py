@@ -175,3 +175,23 @@ def test_thresholds_roundtrip_and_environment():
                          cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     assert out.returncode == 0, out.stderr
     assert out.stdout.strip() == str({"ntt": 512, "poseidon2": 0, "merkle": 64, "fri": 0})
+
+
+@pytest.mark.parametrize("field,p2w", [(0, 16), (1, 16), (1, 12)])
+def test_compress_matches_oracle(oracle, field, p2w):
+    """zkb_mmcs_compress (host-side, no device): TruncatedPermutation of digest pairs."""
+    import numpy as np
+
+    import ziros_b200 as Z
+    from conftest import rand_field
+
+    mmcs = Z.CudaMerkleTreeMmcs(field, 42, p2w)
+    d = mmcs.digest_elems
+    left, right = rand_field(field, (5, d), 1), rand_field(field, (5, d), 2)
+    got = mmcs.compress(left, right)
+    h = oracle.hasher(field, 42, p2w)
+    assert np.array_equal(got, np.stack([oracle.compress(h, a, b) for a, b in zip(left, right)]))
+    with pytest.raises(Z.ZkbError):
+        bad = left.copy()
+        bad[0, 0] = 0x78000001 if field == 0 else 0xFFFFFFFF00000001
+        mmcs.compress(bad, right)

@@ -183,6 +183,8 @@ SIGNATURES = {
     "zkb_challenger_sample": (_I, [_P, _P, _SZ]),
     "zkb_challenger_sample_bits": (_I, [_P, _U32, _P]),
     "zkb_challenger_free": (None, [_P]),
+    "zkb_fri_commit_babybear_ext4_challenger_dev": (_I, [_P, _P, _P, _P, _P, _P]),
+    "zkb_mmcs_compress": (_I, [_P, _P, _P, _SZ, _P]),
     "zkb_batch_create": (_I, [_P, _P, _SZ, _P, _P]),
     "zkb_batch_trace_ptr": (_I, [_P, _SZ, _P]),
     "zkb_batch_copy_in": (_I, [_P, _SZ, _P, _I, _P]),

@@ -263,6 +263,17 @@ class CudaMerkleTreeMmcs:
         N.check(rc)
         return True
 
+    def compress(self, left, right) -> np.ndarray:
+        """TruncatedPermutation of digest pairs (host): left, right (n, OUT) -> (n, OUT)."""
+        dt = dtype_of(self.field)
+        lt = np.ascontiguousarray(left, dtype=dt).reshape(-1, self.digest_elems)
+        rt = np.ascontiguousarray(right, dtype=dt).reshape(-1, self.digest_elems)
+        if lt.shape != rt.shape:
+            raise ValueError("left and right hold different numbers of digests")
+        out = np.zeros_like(lt)
+        N.check(N.load().zkb_mmcs_compress(C.byref(self.hasher), _ptr(lt), _ptr(rt), lt.shape[0], _ptr(out)))
+        return out
+
     def open_batch(self, index: int, tree: Tree) -> Tuple[List[np.ndarray], List[np.ndarray]]:
         """Mmcs::open_batch -> (rows per matrix, sibling digests)."""
         dt = dtype_of(self.field)
@@ -475,14 +486,22 @@ class CudaFriProver:
         N.check(N.load().zkb_fri_commit_babybear_ext4(C.byref(self.hasher), C.byref(prm), _ptr(cw), C.byref(h)))
         return FriProof(h, prm)
 
-    def commit_dev(self, codeword) -> FriProof:
-        """codeword: CUDA tensor of 2^log_n x 4 int32 (extension coefficients)."""
+    def commit_dev(self, codeword, challenger: Optional["Challenger"] = None) -> FriProof:
+        """codeword: CUDA tensor of 2^log_n x 4 int32 (extension coefficients).  With a
+        challenger, the challenges come from it (its state advanced by the call), as when
+        one transcript runs from the trace commitment into FRI."""
         log_n = codeword.shape[0].bit_length() - 1
         prm = self._params(log_n)
         ptr, stream = _torch_ptr_stream(codeword)
         h = C.c_void_p()
-        N.check(N.load().zkb_fri_commit_babybear_ext4_dev(C.byref(self.hasher), C.byref(prm), ptr,
-                                                          C.byref(h), stream))
+        lib = N.load()
+        if challenger is None:
+            N.check(lib.zkb_fri_commit_babybear_ext4_dev(C.byref(self.hasher), C.byref(prm), ptr, C.byref(h),
+                                                         stream))
+        else:
+            prm.transcript = 1
+            N.check(lib.zkb_fri_commit_babybear_ext4_challenger_dev(C.byref(self.hasher), C.byref(prm), ptr,
+                                                                    challenger._h, C.byref(h), stream))
         return FriProof(h, prm)
 
 

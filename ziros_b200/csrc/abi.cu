@@ -650,6 +650,23 @@ int zkb_fri_commit_babybear_ext4_dev(const zkb_hasher *hasher, const zkb_fri_par
   return fri_commit_impl(hasher, params, d_codeword, proof_out, resolve_stream(stream));
 }
 
+int zkb_fri_commit_babybear_ext4_challenger_dev(const zkb_hasher *hasher, const zkb_fri_params *params,
+                                                const uint32_t *d_codeword, zkb_challenger *challenger,
+                                                zkb_fri_proof **proof_out, void *stream) {
+  ZKB_ENTRY();
+  ZKB_REQUIRE(d_codeword != nullptr && challenger != nullptr && params != nullptr && proof_out != nullptr,
+              "null arguments");
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(spec.field == FIELD_BABYBEAR && challenger->c.spec.field == FIELD_BABYBEAR,
+              "the FRI commit phase runs over BabyBear^4");
+  auto pf = std::make_unique<zkb_fri_proof>();
+  ZKB_TRY(fri_commit_ext4_dev(spec, d_codeword, (int)params->log_n, (int)params->log_final, 0,
+                              (int)params->num_queries, 0, &pf->f, resolve_stream(stream), &challenger->c));
+  *proof_out = pf.release();
+  return ZKB_OK;
+}
+
 int zkb_fri_commit_babybear_ext4(const zkb_hasher *hasher, const zkb_fri_params *params,
                                  const uint32_t *codeword, zkb_fri_proof **proof_out) {
   ZKB_ENTRY();

@@ -76,10 +76,6 @@ uint64_t DuplexChallenger::sample_bits(int bits) {
 
 using namespace zkb;
 
-struct zkb_challenger {
-  DuplexChallenger c;
-};
-
 extern "C" {
 
 int zkb_challenger_create(const zkb_hasher *hasher, zkb_challenger **out) {

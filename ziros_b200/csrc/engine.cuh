@@ -152,3 +152,7 @@ struct zkb_tree {
 struct zkb_fri_proof {
   zkb::FriProof f;
 };
+
+struct zkb_challenger {
+  zkb::DuplexChallenger c;
+};

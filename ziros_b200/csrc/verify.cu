@@ -120,10 +120,38 @@ int verify_impl(const HasherSpec &spec, const void *root_v, const uint64_t *heig
   return ZKB_OK;
 }
 
+template <class F, int W>
+int compress_impl(const HasherSpec &spec, const void *left, const void *right, size_t n, void *out) {
+  using T = typename F::T;
+  constexpr int OUT = HostHasher<F, W>::OUT;
+  HostHasher<F, W> h;
+  ZKB_REQUIRE((build_p2_params<F, W>(spec, &h.p)), "invalid Poseidon2 parameters");
+  const T *l = (const T *)left, *r = (const T *)right;
+  for (size_t k = 0; k < n * OUT; k++)
+    ZKB_REQUIRE(l[k] < F::P && r[k] < F::P, "digest element %zu is not canonical", k);
+  for (size_t i = 0; i < n; i++) h.compress(l + i * OUT, r + i * OUT, (T *)out + i * OUT);
+  return ZKB_OK;
+}
+
 }  // namespace
 }  // namespace zkb
 
 using namespace zkb;
+
+extern "C" int zkb_mmcs_compress(const zkb_hasher *hasher, const void *left, const void *right, size_t n,
+                                 void *out) {
+  clear_error();
+  ZKB_REQUIRE(hasher && ((left && right && out) || n == 0), "null arguments");
+  HasherSpec spec;
+  if (!make_hasher_spec(hasher->field, (int)hasher->width, hasher->seed, &spec)) {
+    set_error("unsupported Poseidon2 hasher: field %d width %u", hasher->field, hasher->width);
+    return ZKB_ERR_UNSUPPORTED;
+  }
+  if (n == 0) return ZKB_OK;
+  if (spec.field == FIELD_BABYBEAR) return compress_impl<BabyBear, 16>(spec, left, right, n, out);
+  if (spec.width == 16) return compress_impl<Goldilocks, 16>(spec, left, right, n, out);
+  return compress_impl<Goldilocks, 12>(spec, left, right, n, out);
+}
 
 extern "C" int zkb_mmcs_verify_batch(const zkb_hasher *hasher, const void *root, const uint64_t *heights,
                                      const uint64_t *widths, size_t n_mats, uint64_t index, const void *rows,
