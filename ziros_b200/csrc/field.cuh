@@ -86,10 +86,31 @@ struct Goldilocks {
     return x >= P ? x - P : x;
   }
   __host__ __device__ __forceinline__ static uint64_t add(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+    // One carry chain: s = a + b (carry c), t = s + EPS (carry d).  The sum is >= p
+    // exactly when c or d is set (a + b >= 2^64, or s >= 2^64 - EPS = p), and then the
+    // answer is t: s - p when a + b < 2^64, and s + 2^64 - p (no second carry: s stays
+    // below 2^64 - 2^33 + 1) when it overflowed.  For canonical a, b.
+    uint32_t lo, hi;
+    asm("{\n\t.reg .u32 s0, s1, t0, t1, c;\n\t.reg .pred q;\n\t"
+        "add.cc.u32 s0, %2, %4;\n\t"
+        "addc.cc.u32 s1, %3, %5;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "add.cc.u32 t0, s0, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 t1, s1, 0;\n\t"
+        "addc.u32 c, c, 0;\n\t"
+        "setp.ne.u32 q, c, 0;\n\t"
+        "selp.u32 %0, t0, s0, q;\n\t"
+        "selp.u32 %1, t1, s1, q;\n\t}"
+        : "=r"(lo), "=r"(hi)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)hi << 32) | lo;
+#else
     uint64_t s = a + b;
     // carry out of 2^64: 2^64 = EPS (mod p); the sum of two canonical values stays < 2^64 after it
     if (s < a) s += EPS;
     return canon(s);
+#endif
   }
   __host__ __device__ __forceinline__ static uint64_t sub(uint64_t a, uint64_t b) {
     uint64_t d = a - b;
