@@ -431,14 +431,22 @@ ZKB_API void zkb_rt_free(zkb_rt *rt);
 /* Continuous-batching engine for commit jobs (the role of the reference's proof-level
  * scheduler, zkf-metal/src/batch_prover.rs:94-140, and its bounded in-flight pipeline,
  * zkf-metal/src/pipeline.rs:23-126).  `slots` worker threads each own a stream; a
- * queued job is admitted when its device-memory estimate fits the HBM budget (FIFO,
- * later smaller jobs may pass a blocked head), runs with its LDE, trees and FRI layers
+ * queued job is admitted when its device-memory estimate fits the HBM budget (in the
+ * order `policy` gives), runs with its LDE, trees and FRI layers
  * device-resident, and releases its memory when its answers are on the host.  Jobs on
  * different slots overlap on the GPU; a job's results depend only on its inputs. */
 typedef struct {
   uint32_t slots;        /* concurrent jobs */
   uint64_t hbm_budget;   /* bytes for job state; 0 = free device memory minus 2 GiB */
+  uint32_t policy;       /* admission: ZKB_ADMIT_FIFO or ZKB_ADMIT_SMALLEST */
 } zkb_engine_config;
+/* FIFO: the oldest queued job that fits the remaining budget (a blocked head may be passed
+ * by smaller jobs).  SMALLEST: the fitting job with the fewest trace cells, except that a
+ * job passed over ZKB_ADMIT_MAX_BYPASS times is admitted next, and while it does not fit
+ * nothing else is admitted (no job waits forever). */
+#define ZKB_ADMIT_FIFO 0
+#define ZKB_ADMIT_SMALLEST 1
+#define ZKB_ADMIT_MAX_BYPASS 8
 typedef struct {
   zkb_hasher hasher;
   const void *trace;     /* host memory (pinned for full copy bandwidth), valid until done */

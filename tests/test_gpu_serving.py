@@ -112,3 +112,63 @@ def test_job_log_lines_and_nvtx_ranges(tmp_path):
     lines = [json.loads(x) for x in log.read_text().splitlines()]
     assert sorted((d["log_h"], d["width"]) for d in lines) == [(10, 16), (12, 24)]
     assert all(d["status"] == 0 and d["latency_ms"] >= d["run_ms"] >= 0 for d in lines)
+
+
+def test_smallest_policy_results_identical_to_alone():
+    jobs = _jobs()
+    solo = Z.CommitEngine(slots=1)
+    alone = _run(solo, jobs, concurrent=False)
+    solo.close()
+    eng = Z.CommitEngine(slots=3, policy="smallest")
+    mixed = _run(eng, jobs, concurrent=True)
+    eng.close()
+    for (field, trace, fri), a, m in zip(jobs, alone, mixed):
+        assert (a[0] == m[0]).all()
+        if fri:
+            assert (a[1].roots == m[1].roots).all() and (a[1].query_siblings == m[1].query_siblings).all()
+
+
+def _start_order(policy, n_small):
+    """One slot: a long job runs while a medium job and then n_small small jobs queue up;
+    returns the labels in the order the jobs started."""
+    import time
+
+    big = rand_field(0, (1 << 19, 64), 70)
+    medium = rand_field(0, (1 << 16, 32), 71)
+    smalls = [rand_field(0, (1 << 10, 8), 72 + k) for k in range(n_small)]
+    eng = Z.CommitEngine(slots=1, policy=policy)
+    subs = []
+    for label, t in [("big", big), ("medium", medium)] + [(f"small{k}", s) for k, s in enumerate(smalls)]:
+        jid = eng.submit(t, field=0, seed=42, log_blowup=1)
+        subs.append((label, jid, time.perf_counter()))
+        if label == "big":  # the slot takes it before anything else is queued
+            t0 = time.perf_counter()
+            while eng.stats()["queued"] and time.perf_counter() - t0 < 10:
+                time.sleep(0.0002)
+    starts = []
+    for label, jid, t_sub in subs:
+        res = eng.wait(jid)
+        starts.append((t_sub + res[2]["queue_ms"] / 1e3, label))
+    eng.close()
+    return [label for _, label in sorted(starts)]
+
+
+def test_fifo_admits_in_arrival_order():
+    order = _start_order("fifo", 3)
+    assert order == ["big", "medium", "small0", "small1", "small2"]
+
+
+def test_smallest_first_with_bounded_bypass():
+    """The small jobs pass the medium one until it has been passed over
+    ZKB_ADMIT_MAX_BYPASS times; then it goes next."""
+    from ziros_b200 import _native as N
+
+    order = _start_order("smallest", N.ADMIT_MAX_BYPASS + 2)
+    assert order[0] == "big"
+    assert order.index("medium") == 1 + N.ADMIT_MAX_BYPASS
+    assert all(x.startswith("small") for x in order[1:1 + N.ADMIT_MAX_BYPASS])
+
+
+def test_unknown_policy_is_rejected():
+    with pytest.raises(ValueError):
+        Z.CommitEngine(slots=1, policy="lifo")

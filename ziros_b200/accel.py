@@ -517,10 +517,17 @@ class CommitEngine:
     """Continuous-batching commit engine (zkb_engine_*): jobs are submitted without
     blocking, admitted by free HBM and slot, and overlap on the device."""
 
-    def __init__(self, slots: int = 2, hbm_budget: int = 0):
+    POLICIES = {"fifo": N.ADMIT_FIFO, "smallest": N.ADMIT_SMALLEST}
+
+    def __init__(self, slots: int = 2, hbm_budget: int = 0, policy: str = "fifo"):
+        """policy "fifo": oldest fitting job first; "smallest": fewest cells first, a job
+        passed over ADMIT_MAX_BYPASS times goes next."""
         lib = N.load()
         self._h = C.c_void_p()
-        N.check(lib.zkb_engine_create(C.byref(N.EngineConfig(slots, hbm_budget)), C.byref(self._h)))
+        if policy not in self.POLICIES:
+            raise ValueError(f"unknown admission policy {policy!r}")
+        cfg = N.EngineConfig(slots, hbm_budget, self.POLICIES[policy])
+        N.check(lib.zkb_engine_create(C.byref(cfg), C.byref(self._h)))
         self._keep = {}
 
     def submit(self, trace, field: int = BABYBEAR, seed: int = 42, log_blowup: int = 1, p2_width: int = 16,

@@ -378,10 +378,17 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
     ZKB_TRY(staged.alloc(n * width * es, s));
     if (upload_mu) {
       // one upload at a time: concurrent jobs would split the PCIe link and all start
-      // computing late; serialised, each upload runs under the other jobs' kernels
-      std::lock_guard<std::mutex> lk(*upload_mu);
-      ZKB_CHECK_CUDA(cudaMemcpyAsync(staged.p, h_trace, n * width * es, cudaMemcpyHostToDevice, s));
-      ZKB_TRY(wait_stream(s));
+      // computing late; serialised, each upload runs under the other jobs' kernels.  The
+      // token is taken per 256 MiB piece, so a small job's upload waits for one piece of
+      // a large job's, not for all of it.
+      const size_t total = n * width * es, piece = 256ull << 20;
+      for (size_t off = 0; off < total; off += piece) {
+        const size_t len = total - off < piece ? total - off : piece;
+        std::lock_guard<std::mutex> lk(*upload_mu);
+        ZKB_CHECK_CUDA(cudaMemcpyAsync((char *)staged.p + off, (const char *)h_trace + off, len,
+                                       cudaMemcpyHostToDevice, s));
+        ZKB_TRY(wait_stream(s));
+      }
     } else {
       ZKB_CHECK_CUDA(cudaMemcpyAsync(staged.p, h_trace, n * width * es, cudaMemcpyHostToDevice, s));
     }

@@ -44,10 +44,14 @@ void clear_error();
     }                                    \
   } while (0)
 
-// A cached device table (twiddles, coset factors).  Owned by the context.
+// A cached device table (twiddles, coset factors).  Owned by the context.  It is built
+// on the stream of the call that first needed it; `ready` is recorded after the build, and
+// every later user's stream waits for it, so no host thread waits for a build.
 struct DeviceTable {
   void *ptr = nullptr;
   size_t bytes = 0;
+  cudaEvent_t ready = nullptr;
+  bool complete = false;  // `ready` seen complete: later users need not wait
 };
 
 // One per CUDA device: caches shared by every stream on that device.

@@ -75,6 +75,45 @@ static constexpr int field_id() {
   return sizeof(typename F::T) == 4 ? ZKB_FIELD_BABYBEAR : ZKB_FIELD_GOLDILOCKS;
 }
 
+// A cached table for use on stream s (context lock held): s waits for the table's build.
+// Inside a graph capture the wait is captured as a wait on an external event, which is a
+// no-op once the build has finished.
+static int table_use(DeviceTable &t, cudaStream_t s) {
+  if (t.complete || !t.ready) return ZKB_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  ZKB_CHECK_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    ZKB_CHECK_CUDA(cudaStreamWaitEvent(s, t.ready, cudaEventWaitExternal));
+    return ZKB_OK;
+  }
+  const cudaError_t q = cudaEventQuery(t.ready);
+  if (q == cudaSuccess) {
+    t.complete = true;
+    return ZKB_OK;
+  }
+  if (q != cudaErrorNotReady) ZKB_CHECK_CUDA(q);
+  ZKB_CHECK_CUDA(cudaStreamWaitEvent(s, t.ready, 0));
+  return ZKB_OK;
+}
+
+// A table is built on the stream that first needs it, never inside a graph capture (the
+// capture would own its memory).
+static int table_build_allowed(cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  ZKB_CHECK_CUDA(cudaStreamIsCapturing(s, &cs));
+  ZKB_REQUIRE(cs == cudaStreamCaptureStatusNone,
+              "NTT tables for this shape are built on first use, which cannot happen inside a graph "
+              "capture: run the shape once before capturing");
+  return ZKB_OK;
+}
+
+// Publishes a table whose build was just enqueued on s.
+static int table_publish(DeviceTable &t, cudaStream_t s) {
+  ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming));
+  ZKB_CHECK_CUDA(cudaEventRecord(t.ready, s));
+  return ZKB_OK;
+}
+
 template <class F>
 int get_twiddles(int log_n, bool inverse, const typename F::T **out, cudaStream_t s) {
   using T = typename F::T;
@@ -88,21 +127,24 @@ int get_twiddles(int log_n, bool inverse, const typename F::T **out, cudaStream_
   auto key = std::make_tuple(field_id<F>(), log_n, (int)inverse);
   auto it = ctx->twiddles.find(key);
   if (it != ctx->twiddles.end()) {
+    ZKB_TRY(table_use(it->second, s));
     *out = (const T *)it->second.ptr;
     return ZKB_OK;
   }
+  ZKB_TRY(table_build_allowed(s));
   uint64_t n = 1ull << log_n;
   void *p = nullptr;
-  ZKB_CHECK_CUDA(cudaMalloc(&p, n * sizeof(T)));
+  ZKB_TRY(dev_alloc(&p, n * sizeof(T), s));
   T w = two_adic_generator<F>(log_n);
   if (inverse) w = inv_host<F>(w);
+  DeviceTable t{p, n * sizeof(T)};
   int rc = launch_powers<F>((T *)p, n, w, 1, s);
-  if (rc == ZKB_OK) rc = wait_stream(s);
+  if (rc == ZKB_OK) rc = table_publish(t, s);
   if (rc != ZKB_OK) {
-    cudaFree(p);
+    cudaFreeAsync(p, s);
     return rc;
   }
-  ctx->twiddles[key] = DeviceTable{p, n * sizeof(T)};
+  ctx->twiddles[key] = t;
   *out = (const T *)p;
   return ZKB_OK;
 }
@@ -118,12 +160,14 @@ static int get_coset_table(int log_n, int log_b, typename F::T shift, const type
   auto key = std::make_tuple(field_id<F>(), log_n, log_b, (uint64_t)shift);
   auto it = ctx->cosets.find(key);
   if (it != ctx->cosets.end()) {
+    ZKB_TRY(table_use(it->second, s));
     *out = (const T *)it->second.ptr;
     return ZKB_OK;
   }
+  ZKB_TRY(table_build_allowed(s));
   uint64_t n = 1ull << log_n, b = 1ull << log_b;
   void *p = nullptr;
-  ZKB_CHECK_CUDA(cudaMalloc(&p, n * b * sizeof(T)));
+  ZKB_TRY(dev_alloc(&p, n * b * sizeof(T), s));
   T w_bn = two_adic_generator<F>(log_n + log_b);
   T n_inv = inv_host<F>((T)(n % (uint64_t)F::P));
   T wj = 1;
@@ -132,12 +176,13 @@ static int get_coset_table(int log_n, int log_b, typename F::T shift, const type
     rc = launch_powers<F>((T *)p + j * n, n, F::mul_host(shift, wj), n_inv, s);
     wj = F::mul_host(wj, w_bn);
   }
-  if (rc == ZKB_OK) rc = wait_stream(s);
+  DeviceTable t{p, n * b * sizeof(T)};
+  if (rc == ZKB_OK) rc = table_publish(t, s);
   if (rc != ZKB_OK) {
-    cudaFree(p);
+    cudaFreeAsync(p, s);
     return rc;
   }
-  ctx->cosets[key] = DeviceTable{p, n * b * sizeof(T)};
+  ctx->cosets[key] = t;
   *out = (const T *)p;
   return ZKB_OK;
 }
@@ -174,16 +219,18 @@ static int get_fused_tables(int log_n, int log_b, typename F::T shift, int K, co
   const uint64_t n = 1ull << log_n;
   auto it = ctx->fused.find(key);
   if (it == ctx->fused.end()) {
+    // ctab and ftw come from get_coset_table / get_twiddles on this stream, which made s
+    // wait for their builds
+    ZKB_TRY(table_build_allowed(s));
     void *p = nullptr;
-    ZKB_CHECK_CUDA(cudaMalloc(&p, ((n << log_b) + n) * sizeof(T)));
+    ZKB_TRY(dev_alloc(&p, ((n << log_b) + n) * sizeof(T), s));
     T *ct = (T *)p, *ft = ct + (n << log_b);
     ZKB_LAUNCH("table_fused", s, fused_tables_kernel<F><<<grid_for((n << log_b) + n, 256), 256, 0, s>>>(ctab, ftw, log_n, K, log_b, ct, ft));
-    const int rc = wait_stream(s);
-    if (rc != ZKB_OK) {
-      cudaFree(p);
-      return rc;
-    }
-    it = ctx->fused.emplace(key, DeviceTable{p, ((n << log_b) + n) * sizeof(T)}).first;
+    DeviceTable t{p, ((n << log_b) + n) * sizeof(T)};
+    ZKB_TRY(table_publish(t, s));
+    it = ctx->fused.emplace(key, t).first;
+  } else {
+    ZKB_TRY(table_use(it->second, s));
   }
   *ctab_t = (const T *)it->second.ptr;
   *ftw_t = *ctab_t + (n << log_b);

@@ -2,8 +2,9 @@
 //
 // Jobs (a host trace to commit, optionally followed by the FRI commit phase on the
 // alpha-reduced LDE) are submitted without blocking.  `slots` worker threads each
-// own a CUDA stream; a worker admits the first queued job whose device-memory
-// estimate fits what is left of the HBM budget (FIFO with backfill), copies the trace
+// own a CUDA stream; a worker admits a queued job whose device-memory estimate fits
+// what is left of the HBM budget (the oldest such job, or with ZKB_ADMIT_SMALLEST the
+// one with the fewest cells, under a bound on how often a job is passed over), copies the trace
 // in on its stream, keeps the LDE, the trees and the FRI layers device-resident until
 // the job's answers are on the host, then releases the memory and wakes the queue.
 // Jobs on different workers overlap on the GPU (one job's copy under another's
@@ -55,6 +56,7 @@ struct Job {
   HasherSpec spec;
   uint64_t mem_estimate = 0;
   Clock::time_point t_submit, t_start, t_done;
+  uint32_t bypassed = 0;  // times a younger job was admitted while this one waited
   int status = 1;  // 1 queued / running, 0 done, <0 error
   std::string error;
   uint32_t root[16] = {0};
@@ -95,6 +97,7 @@ uint64_t job_bytes(const zkb_job_desc &d) {
 struct zkb_engine {
   int device = 0;
   uint64_t budget = 0, in_use = 0;
+  uint32_t policy = ZKB_ADMIT_FIFO;
   std::mutex mu;
   std::mutex upload_mu;  // one job's trace crosses PCIe at a time
   std::condition_variable cv_queue, cv_done;
@@ -104,6 +107,24 @@ struct zkb_engine {
   uint64_t next_id = 1;
   bool stopping = false;
   uint64_t completed = 0, peak_in_use = 0;
+
+  static uint64_t cells(const Job &j) { return ((uint64_t)j.desc.width) << j.desc.log_h; }
+
+  // The queued job to admit now (queue.end(): none).  Called with mu held.
+  std::deque<std::shared_ptr<Job>>::iterator pick() {
+    auto fits = [&](const std::shared_ptr<Job> &j) { return in_use + j->mem_estimate <= budget; };
+    if (policy != ZKB_ADMIT_SMALLEST) {
+      auto it = queue.begin();
+      while (it != queue.end() && !fits(*it)) ++it;
+      return it;
+    }
+    auto best = queue.end();
+    for (auto it = queue.begin(); it != queue.end(); ++it) {
+      if ((*it)->bypassed >= ZKB_ADMIT_MAX_BYPASS) return fits(*it) ? it : queue.end();  // it goes next
+      if (fits(*it) && (best == queue.end() || cells(**it) < cells(**best))) best = it;
+    }
+    return best;
+  }
 
   void worker_loop() {
     cudaSetDevice(device);
@@ -115,11 +136,11 @@ struct zkb_engine {
         std::unique_lock<std::mutex> lk(mu);
         for (;;) {
           if (stopping && queue.empty()) break;
-          auto it = queue.begin();
-          for (; it != queue.end(); ++it)
-            if (in_use + (*it)->mem_estimate <= budget) break;
+          auto it = pick();
           if (it != queue.end()) {
             job = *it;
+            // every older job still queued was passed over once more
+            for (auto o = queue.begin(); o != it; ++o) (*o)->bypassed++;
             queue.erase(it);
             in_use += job->mem_estimate;
             peak_in_use = in_use > peak_in_use ? in_use : peak_in_use;
@@ -186,6 +207,9 @@ int zkb_engine_create(const zkb_engine_config *cfg, zkb_engine **out) {
   const uint64_t reserve = 2ull << 30;
   const uint64_t avail = free_b + pool_idle > reserve ? free_b + pool_idle - reserve : 0;
   e->budget = cfg->hbm_budget ? (cfg->hbm_budget < avail ? cfg->hbm_budget : avail) : avail;
+  ZKB_REQUIRE(cfg->policy == ZKB_ADMIT_FIFO || cfg->policy == ZKB_ADMIT_SMALLEST, "unknown admission policy %u",
+              cfg->policy);
+  e->policy = cfg->policy;
   zkb_engine *raw = e.get();
   for (uint32_t i = 0; i < cfg->slots; i++) e->workers.emplace_back([raw] { raw->worker_loop(); });
   *out = e.release();
