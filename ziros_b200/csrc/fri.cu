@@ -113,29 +113,99 @@ struct Ext4Params {
   uint32_t inv2_enc;
 };
 
+// Output i of the fold from the rows r0 = e[2i], r1 = e[2i+1] (n_out = 2^log_n outputs).
+__device__ __forceinline__ uint4 fold_ext4_one(uint4 r0, uint4 r1, uint64_t i, int log_n, const Ext4Params &prm,
+                                               const uint32_t *__restrict__ itw) {
+  using B = BabyBear;
+  uint64_t r = log_n ? (__brevll(i) >> (64 - log_n)) : 0;
+  const uint32_t w = itw[r];
+  Ext4 d;
+  d.c[0] = B::mul_tw(B::sub(r0.x, r1.x), w);
+  d.c[1] = B::mul_tw(B::sub(r0.y, r1.y), w);
+  d.c[2] = B::mul_tw(B::sub(r0.z, r1.z), w);
+  d.c[3] = B::mul_tw(B::sub(r0.w, r1.w), w);
+  Ext4 t = ext4_mul_enc(d, prm.half_beta_enc);
+  uint4 o;
+  o.x = B::add(B::mul_tw(B::add(r0.x, r1.x), prm.inv2_enc), t.c[0]);
+  o.y = B::add(B::mul_tw(B::add(r0.y, r1.y), prm.inv2_enc), t.c[1]);
+  o.z = B::add(B::mul_tw(B::add(r0.z, r1.z), prm.inv2_enc), t.c[2]);
+  o.w = B::add(B::mul_tw(B::add(r0.w, r1.w), prm.inv2_enc), t.c[3]);
+  return o;
+}
+
 __global__ void fri_fold_ext4_kernel(const uint32_t *__restrict__ e, uint32_t *__restrict__ out,
                                      uint64_t n_out, int log_n, const Ext4Params prm,
                                      const uint32_t *__restrict__ itw) {
-  using B = BabyBear;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_out;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint4 r0 = reinterpret_cast<const uint4 *>(e)[2 * i];
     const uint4 r1 = reinterpret_cast<const uint4 *>(e)[2 * i + 1];
-    uint64_t r = log_n ? (__brevll(i) >> (64 - log_n)) : 0;
-    const uint32_t w = itw[r];
-    Ext4 d;
-    d.c[0] = B::mul_tw(B::sub(r0.x, r1.x), w);
-    d.c[1] = B::mul_tw(B::sub(r0.y, r1.y), w);
-    d.c[2] = B::mul_tw(B::sub(r0.z, r1.z), w);
-    d.c[3] = B::mul_tw(B::sub(r0.w, r1.w), w);
-    Ext4 t = ext4_mul_enc(d, prm.half_beta_enc);
-    uint4 o;
-    o.x = B::add(B::mul_tw(B::add(r0.x, r1.x), prm.inv2_enc), t.c[0]);
-    o.y = B::add(B::mul_tw(B::add(r0.y, r1.y), prm.inv2_enc), t.c[1]);
-    o.z = B::add(B::mul_tw(B::add(r0.z, r1.z), prm.inv2_enc), t.c[2]);
-    o.w = B::add(B::mul_tw(B::add(r0.w, r1.w), prm.inv2_enc), t.c[3]);
-    reinterpret_cast<uint4 *>(out)[i] = o;
+    reinterpret_cast<uint4 *>(out)[i] = fold_ext4_one(r0, r1, i, log_n, prm, itw);
   }
+}
+
+// The next FRI layer's leaves while it is made.  Leaf j of a layer is the sponge digest
+// of its codeword's rows 2j and 2j+1 flattened to 8 base elements (one permutation);
+// with FOLD each thread first folds its four input rows 4j..4j+3 (the two pairs that
+// become rows 2j and 2j+1) and stores them, so the new codeword is hashed from
+// registers instead of being read back.  Without FOLD it hashes the codeword `e` itself
+// (round 0).  n_leaves = 2^(log_out - 1), the output codeword holding 2^log_out rows.
+template <bool FOLD>
+__global__ void __launch_bounds__(128)
+    fri_fold_hash_kernel(const uint32_t *__restrict__ e, uint32_t *__restrict__ out, uint64_t n_leaves, int log_out,
+                         const Ext4Params prm, const uint32_t *__restrict__ itw, uint32_t *__restrict__ digests,
+                         const __grid_constant__ P2Params<BabyBear, 16> p) {
+  using D = Dom<BabyBear>;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n_leaves;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 *in = reinterpret_cast<const uint4 *>(e);
+    uint4 a, b;
+    if constexpr (FOLD) {
+      a = fold_ext4_one(in[4 * j], in[4 * j + 1], 2 * j, log_out, prm, itw);
+      b = fold_ext4_one(in[4 * j + 2], in[4 * j + 3], 2 * j + 1, log_out, prm, itw);
+      reinterpret_cast<uint4 *>(out)[2 * j] = a;
+      reinterpret_cast<uint4 *>(out)[2 * j + 1] = b;
+    } else {
+      a = in[2 * j];
+      b = in[2 * j + 1];
+    }
+    uint32_t st[16] = {D::enter(a.x), D::enter(a.y), D::enter(a.z), D::enter(a.w),
+                       D::enter(b.x), D::enter(b.y), D::enter(b.z), D::enter(b.w), 0, 0, 0, 0, 0, 0, 0, 0};
+    p2_permute<BabyBear, 16>(st, p);
+    uint4 *dg = reinterpret_cast<uint4 *>(digests) + 2 * j;
+    dg[0] = make_uint4(D::leave(st[0]), D::leave(st[1]), D::leave(st[2]), D::leave(st[3]));
+    dg[1] = make_uint4(D::leave(st[4]), D::leave(st[5]), D::leave(st[6]), D::leave(st[7]));
+  }
+}
+
+static int fold_params(const uint32_t beta[4], Ext4Params *prm) {
+  const uint32_t inv2 = inv_host<BabyBear>(2);
+  for (int k = 0; k < 4; k++) {
+    ZKB_REQUIRE(beta[k] < BabyBear::P, "beta is not canonical");
+    prm->half_beta_enc.c[k] = BabyBear::tw_encode(BabyBear::mul_host(beta[k], inv2));
+  }
+  prm->inv2_enc = BabyBear::tw_encode(inv2);
+  return ZKB_OK;
+}
+
+// Leaves of the layer whose codeword (2^log_out rows) is cw_out: folded from cw_in with
+// beta (stored into cw_out as well), or, with beta NULL, hashed from cw_in = cw_out.
+static int fri_fold_hash_dev(const uint32_t *cw_in, uint32_t *cw_out, int log_out, const uint32_t *beta,
+                             uint32_t *leaf_digests, const P2Params<BabyBear, 16> &p, cudaStream_t s) {
+  const uint64_t n_leaves = 1ull << (log_out - 1);
+  DeviceContext *ctx;
+  ZKB_TRY(current_context(&ctx));
+  const unsigned grid = grid_for(n_leaves, 128, (unsigned)ctx->sm_count * 16u);
+  if (beta) {
+    Ext4Params prm;
+    ZKB_TRY(fold_params(beta, &prm));
+    const uint32_t *itw;
+    ZKB_TRY(get_twiddles<BabyBear>(log_out + 1, true, &itw, s));
+    ZKB_LAUNCH("fri_fold_hash", s, fri_fold_hash_kernel<true><<<grid, 128, 0, s>>>(cw_in, cw_out, n_leaves, log_out, prm, itw, leaf_digests, p));
+  } else {
+    ZKB_LAUNCH("fri_leaf_hash", s, fri_fold_hash_kernel<false><<<grid, 128, 0, s>>>(cw_in, nullptr, n_leaves, log_out, Ext4Params{}, nullptr, leaf_digests, p));
+  }
+  return ZKB_OK;
 }
 
 int fri_fold_ext4_dev(const uint32_t *d_evals, size_t n_out, const uint32_t beta[4],
@@ -146,12 +216,7 @@ int fri_fold_ext4_dev(const uint32_t *d_evals, size_t n_out, const uint32_t beta
   ZKB_REQUIRE(((uintptr_t)d_evals & 15) == 0 && ((uintptr_t)d_out & 15) == 0,
               "extension buffers must be 16-byte aligned");
   Ext4Params prm;
-  const uint32_t inv2 = inv_host<BabyBear>(2);
-  for (int k = 0; k < 4; k++) {
-    ZKB_REQUIRE(beta[k] < BabyBear::P, "beta is not canonical");
-    prm.half_beta_enc.c[k] = BabyBear::tw_encode(BabyBear::mul_host(beta[k], inv2));
-  }
-  prm.inv2_enc = BabyBear::tw_encode(inv2);
+  ZKB_TRY(fold_params(beta, &prm));
   const uint32_t *itw;
   ZKB_TRY(get_twiddles<BabyBear>(log_n + 1, true, &itw, s));
   ZKB_LAUNCH("fri_fold_ext4", s, fri_fold_ext4_kernel<<<grid_for(n_out, 256), 256, 0, s>>>(d_evals, d_out, n_out, log_n, prm, itw));
@@ -238,10 +303,10 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
   pf->log_final = log_final;
   const int rounds = log_n - log_final;
   ZKB_REQUIRE(!ch || ch->spec.field == FIELD_BABYBEAR, "the transcript must be over BabyBear");
-  // Seeded challenges: every fold can run before any layer is hashed, so all rounds'
-  // folds run first and the trees of all rounds are hashed together (one leaf launch,
-  // one launch per tree level across the rounds, one root gather).  Transcript
-  // challenges: beta_r depends on round r's root, so the rounds run in order.
+  // Seeded challenges: every beta is known up front, so the folds (each hashing the
+  // leaves of the layer it makes) run back to back and the trees of all rounds are then
+  // compressed together (one launch per tree level across the rounds, one root gather).
+  // Transcript challenges: beta_r depends on round r's root, so the rounds run in order.
   pf->query_idx.resize(num_queries);
   if (!ch) {
     SmallRng rng(challenge_seed);
@@ -307,10 +372,18 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
     rows[r] = 1ull << (log_n - r - 1);
     layers[r] = base + layers_base + lay_off[r] * 32;
   }
+  // Leaves: layer 0's are hashed from the input codeword; every later layer's leaves are
+  // hashed by the kernel that folds the previous codeword into it (fri_fold_hash_dev),
+  // so no codeword is read back to be hashed.  The last fold (into the final codeword)
+  // has no layer after it.
   std::vector<std::vector<uint64_t>> layer_len(rounds);
+  auto leaves = [&](int r) { return (uint32_t *)layers[r]; };
+  ZKB_TRY(fri_fold_hash_dev(cw(0), nullptr, log_n, nullptr, leaves(0), p, s));
   if (!ch) {
-    for (int r = 0; r < rounds; r++)
-      ZKB_TRY(fri_fold_ext4_dev(cw(r), 1ull << (log_n - r - 1), pf->betas[r].data(), (uint32_t *)cw(r + 1), s));
+    for (int r = 1; r < rounds; r++)
+      ZKB_TRY(fri_fold_hash_dev(cw(r - 1), (uint32_t *)cw(r), log_n - r, pf->betas[r - 1].data(), leaves(r), p, s));
+    ZKB_TRY(fri_fold_ext4_dev(cw(rounds - 1), 1ull << log_final, pf->betas[rounds - 1].data(),
+                              (uint32_t *)cw(rounds), s));
     mt::Tables tab;
     mt::build_tables(data, rows, widths, layers, layers[0], 8, 4, &tab);
     mt::LeafJob *d_leaf;
@@ -318,7 +391,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
     uint64_t *d_root_off;
     ZKB_TRY(mt::upload_tables(tab, base + tables_off, s, &d_leaf, &d_comp, &d_root_off));
     ZKB_TRY((mt::launch_trees<BabyBear, 16>(tab, d_leaf, d_comp, d_root_off, layers[0], base + roots_off, p, 128,
-                                            s, "fri_leaf_hash", "fri_compress", "fri_roots")));
+                                            s, nullptr, "fri_compress", "fri_roots")));
     layer_len = tab.layer_len;
   } else {
     char *tslot = base + tables_off;
@@ -333,14 +406,17 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
       tslot += tab.device_bytes();
       char *d_root = base + roots_off + (size_t)r * 32;
       ZKB_TRY((mt::launch_trees<BabyBear, 16>(tab, d_leaf, d_comp, d_root_off, layers[r], d_root, p, 128, s,
-                                              "fri_leaf_hash", "fri_compress", "fri_roots")));
+                                              nullptr, "fri_compress", "fri_roots")));
       ZKB_CHECK_CUDA(cudaMemcpyAsync(root, d_root, 32, cudaMemcpyDeviceToHost, s));
       ZKB_TRY(wait_stream(s));
       for (uint32_t v : root) ch->observe(v);
       std::array<uint32_t, 4> beta;
       for (auto &b : beta) b = (uint32_t)ch->sample();
       pf->betas.push_back(beta);
-      ZKB_TRY(fri_fold_ext4_dev(cw(r), rows[r], beta.data(), (uint32_t *)cw(r + 1), s));
+      if (r + 1 < rounds)
+        ZKB_TRY(fri_fold_hash_dev(cw(r), (uint32_t *)cw(r + 1), log_n - r - 1, beta.data(), leaves(r + 1), p, s));
+      else
+        ZKB_TRY(fri_fold_ext4_dev(cw(r), 1ull << log_final, beta.data(), (uint32_t *)cw(r + 1), s));
       layer_len[r] = tab.layer_len[0];
     }
   }

@@ -195,7 +195,8 @@ inline int upload_tables(const Tables &t, void *dev, cudaStream_t s, LeafJob **d
   return ZKB_OK;
 }
 
-// Enqueues the leaf hashing, every compression level and the root gather on s.
+// Enqueues the leaf hashing (unless the caller has written every job's leaf digests
+// already: leaf_name NULL), every compression level and the root gather on s.
 template <class F, int W>
 int launch_trees(const Tables &t, const LeafJob *d_leaf, const CompJob *d_comp, const uint64_t *d_root_off,
                  const void *base, void *d_roots, const P2Params<F, W> &p, unsigned leaf_threads,
@@ -205,7 +206,8 @@ int launch_trees(const Tables &t, const LeafJob *d_leaf, const CompJob *d_comp, 
   DeviceContext *ctx;
   ZKB_TRY(current_context(&ctx));
   const int n = (int)t.leaf.size();
-  ZKB_LAUNCH(leaf_name, s, mt_leaf_kernel<F, W><<<grid_for(t.total_rows, leaf_threads, (unsigned)ctx->sm_count * (2048u / leaf_threads)), leaf_threads, n * sizeof(uint64_t), s>>>(d_leaf, n, t.total_rows, p));
+  if (leaf_name)
+    ZKB_LAUNCH(leaf_name, s, mt_leaf_kernel<F, W><<<grid_for(t.total_rows, leaf_threads, (unsigned)ctx->sm_count * (2048u / leaf_threads)), leaf_threads, n * sizeof(uint64_t), s>>>(d_leaf, n, t.total_rows, p));
   for (size_t l = 0; l < t.lvl_cnt.size(); l++) {
     ZKB_LAUNCH(comp_name, s, mt_compress_kernel<F, W><<<grid_for(t.lvl_total[l], 128, (unsigned)ctx->sm_count * 16u), 128, t.lvl_cnt[l] * sizeof(uint64_t), s>>>(d_comp + t.lvl_off[l], (int)t.lvl_cnt[l], t.lvl_total[l], p));
   }
