@@ -51,6 +51,15 @@ struct BabyBear {
     uint64_t u = t + (uint64_t)m * P;
     return (uint32_t)(u >> 32);
   }
+  // (a0*b0 + a1*b1) * 2^-32 in [0, 2p), for canonical operands (the sum stays below
+  // 2p^2 < p*2^32): two products, one reduction.
+  __host__ __device__ __forceinline__ static uint32_t mont_lazy_sum(uint32_t a0, uint32_t b0, uint32_t a1,
+                                                                    uint32_t b1) {
+    uint64_t t = (uint64_t)a0 * b0 + (uint64_t)a1 * b1;
+    uint32_t m = (uint32_t)t * NPINV;
+    uint64_t u = t + (uint64_t)m * P;
+    return (uint32_t)(u >> 32);
+  }
   // t * 2^-32 mod p, canonical, for any t < p*2^32 (e.g. a sum of mont_lazy results).
   __host__ __device__ __forceinline__ static uint32_t mont_reduce(uint64_t t) {
     uint32_t m = (uint32_t)t * NPINV;
@@ -66,6 +75,19 @@ struct BabyBear {
   __host__ __device__ __forceinline__ static uint32_t mul_tw(uint32_t x, uint32_t w_mont) {
     return mont(x, w_mont);
   }
+  // Product by a constant w (canonical) with its Shoup quotient wq = floor(w * 2^32 / p):
+  // q = floor(x * wq / 2^32) underestimates x * w / p by at most 1, so x * w - q * p,
+  // computed mod 2^32, lies in [0, 2p); any x < 2^32.  Two multiplies and a multiply-add
+  // against the three wide-result multiplies of a Montgomery product.
+  __host__ __device__ __forceinline__ static uint32_t mul_shoup(uint32_t x, uint32_t w, uint32_t wq) {
+#ifdef __CUDA_ARCH__
+    const uint32_t q = __umulhi(x, wq);
+#else
+    const uint32_t q = (uint32_t)(((uint64_t)x * wq) >> 32);
+#endif
+    return red(x * w - q * P);
+  }
+  static inline uint32_t shoup_quotient(uint32_t w) { return (uint32_t)(((uint64_t)w << 32) / P); }
   // Host-side plain product (tables, constants).
   static inline uint32_t mul_host(uint32_t a, uint32_t b) {
     return (uint32_t)(((uint64_t)a * b) % P);

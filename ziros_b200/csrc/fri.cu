@@ -470,8 +470,8 @@ namespace zkb {
 // columns l, l+32, ... (coalesced; V4 = four consecutive columns per lane with 128-bit
 // loads when the width is a multiple of 4), unrolled so that several loads are in
 // flight per lane.  The powers arrive encoded as alpha^j * 2^64 mod p, so each
-// Montgomery product is v * alpha^j * 2^32 and a lane's unreduced 64-bit sum (below
-// p * 2^32 for any width < 2^30) needs one Montgomery reduction to come out as
+// Montgomery product is v * alpha^j * 2^32 and a lane's unreduced 64-bit sum of them
+// (below p * 2^32 for any width < 2^29) needs one Montgomery reduction to come out as
 // sum v * alpha^j; the 32 lane sums are then added mod p across the warp.
 template <bool V4>
 __global__ void __launch_bounds__(256)
@@ -489,14 +489,19 @@ __global__ void __launch_bounds__(256)
       a2 += B::mont_lazy(v, w.z);
       a3 += B::mont_lazy(v, w.w);
     };
+    // two columns per Montgomery reduction (v0 w0 + v1 w1 < 2p^2 < p 2^32)
+    auto acc2 = [&](uint32_t v0, uint4 w0, uint32_t v1, uint4 w1) {
+      a0 += B::mont_lazy_sum(v0, w0.x, v1, w1.x);
+      a1 += B::mont_lazy_sum(v0, w0.y, v1, w1.y);
+      a2 += B::mont_lazy_sum(v0, w0.z, v1, w1.z);
+      a3 += B::mont_lazy_sum(v0, w0.w, v1, w1.w);
+    };
     if constexpr (V4) {
 #pragma unroll 2
       for (uint32_t j = 4 * lane; j < width; j += 128) {
         const uint4 v = *reinterpret_cast<const uint4 *>(row + j);
-        acc(v.x, apow[j]);
-        acc(v.y, apow[j + 1]);
-        acc(v.z, apow[j + 2]);
-        acc(v.w, apow[j + 3]);
+        acc2(v.x, apow[j], v.y, apow[j + 1]);
+        acc2(v.z, apow[j + 2], v.w, apow[j + 3]);
       }
     } else {
 #pragma unroll 4

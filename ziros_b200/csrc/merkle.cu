@@ -92,20 +92,30 @@ __global__ void __launch_bounds__(128)
     uint32_t s[16];
 #pragma unroll
     for (int i = 0; i < 16; i++) s[i] = 0;
+    // Two columns per reduction: v0*w0 + v1*w1 < 2p^2 < p*2^32 is one Montgomery
+    // reduction's input, so a pair costs two wide multiply-adds and one reduction.
     uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
     const uint32_t *rp = mat + row * width;
     for (uint64_t c = 0; c < width; c += 8) {
 #pragma unroll
-      for (int i = 0; i < 8; i++)
+      for (int i = 0; i < 8; i += 2) {
         if (c + i < width) {
-          const uint32_t v = rp[c + i];
-          const uint4 w = apow[c + i];
-          a0 += B::mont_lazy(v, w.x);
-          a1 += B::mont_lazy(v, w.y);
-          a2 += B::mont_lazy(v, w.z);
-          a3 += B::mont_lazy(v, w.w);
-          s[i] = D::enter(v);
+          const uint32_t v0 = rp[c + i];
+          const uint4 w0 = apow[c + i];
+          s[i] = D::enter(v0);
+          uint32_t v1 = 0;
+          uint4 w1 = make_uint4(0, 0, 0, 0);
+          if (c + i + 1 < width) {
+            v1 = rp[c + i + 1];
+            w1 = apow[c + i + 1];
+            s[i + 1] = D::enter(v1);
+          }
+          a0 += B::mont_lazy_sum(v0, w0.x, v1, w1.x);
+          a1 += B::mont_lazy_sum(v0, w0.y, v1, w1.y);
+          a2 += B::mont_lazy_sum(v0, w0.z, v1, w1.z);
+          a3 += B::mont_lazy_sum(v0, w0.w, v1, w1.w);
         }
+      }
       p2_permute<BabyBear, 16>(s, p);
     }
 #pragma unroll

@@ -260,10 +260,59 @@ struct PassGeom {
   int twist;
 };
 
+// w_64^e, e < 32, for the register DIFs: BabyBear holds the canonical powers and their
+// Shoup quotients (products by these constants are Shoup products), Goldilocks the
+// canonical powers (q unused).
 template <class F>
 struct SmallTw {
-  typename F::T w[32];  // w_64^e, e < 32, encoded for F::mul_tw
+  typename F::T w[32];
+  typename F::T q[32];
 };
+
+// A twiddle staged in shared memory, in the form the kernels multiply by.  The cached
+// tables keep the field's encoded form (Montgomery for BabyBear); staging turns a BabyBear
+// entry into its canonical value and Shoup quotient, so every product by it is a Shoup
+// product (about 1.5x the throughput of a Montgomery product on the integer pipes).
+template <class F>
+struct TwS;
+template <>
+struct TwS<BabyBear> {
+  uint32_t w, q;
+};
+template <>
+struct TwS<Goldilocks> {
+  uint64_t w;
+};
+
+// floor(2^64 / p) for BabyBear is 2 * 2^32 + BB_RECIP_LO.
+constexpr uint32_t BB_RECIP_LO = 0x2222221du;
+
+template <class F>
+__device__ __forceinline__ TwS<F> tw_stage(typename F::T enc);
+template <>
+__device__ __forceinline__ TwS<BabyBear> tw_stage<BabyBear>(uint32_t enc) {
+  const uint32_t w = BabyBear::from_mont(enc);
+  // 2w + hi(w * BB_RECIP_LO) = floor(w * floor(2^64/p) / 2^32) is floor(w 2^32 / p) or one
+  // less; the remainder w 2^32 - q p is below 2p < 2^32, so its value mod 2^32 decides.
+  uint32_t q = 2 * w + __umulhi(w, BB_RECIP_LO);
+  if (0u - q * BabyBear::P >= BabyBear::P) q++;
+  return {w, q};
+}
+template <>
+__device__ __forceinline__ TwS<Goldilocks> tw_stage<Goldilocks>(uint64_t enc) {
+  return {enc};
+}
+
+template <class F>
+__device__ __forceinline__ typename F::T tw_mul(typename F::T x, const TwS<F> &t);
+template <>
+__device__ __forceinline__ uint32_t tw_mul<BabyBear>(uint32_t x, const TwS<BabyBear> &t) {
+  return BabyBear::mul_shoup(x, t.w, t.q);
+}
+template <>
+__device__ __forceinline__ uint64_t tw_mul<Goldilocks>(uint64_t x, const TwS<Goldilocks> &t) {
+  return Goldilocks::mul(x, t.w);
+}
 
 __host__ __device__ constexpr int rev_bits(int x, int bits) {
   int r = 0;
@@ -272,15 +321,16 @@ __host__ __device__ constexpr int rev_bits(int x, int bits) {
 }
 
 // (a - b) * w for the DIF butterfly; BabyBear keeps a - b + p unreduced (< 2p), which
-// the lazy Montgomery product accepts.
+// the Shoup product accepts.
 template <class F>
-__device__ __forceinline__ typename F::T dif_mul(typename F::T a, typename F::T b, typename F::T w);
+__device__ __forceinline__ typename F::T dif_mul(typename F::T a, typename F::T b, typename F::T w,
+                                                 typename F::T wq);
 template <>
-__device__ __forceinline__ uint32_t dif_mul<BabyBear>(uint32_t a, uint32_t b, uint32_t w) {
-  return BabyBear::red(BabyBear::mont_lazy(a - b + BabyBear::P, w));
+__device__ __forceinline__ uint32_t dif_mul<BabyBear>(uint32_t a, uint32_t b, uint32_t w, uint32_t wq) {
+  return BabyBear::mul_shoup(a - b + BabyBear::P, w, wq);
 }
 template <>
-__device__ __forceinline__ uint64_t dif_mul<Goldilocks>(uint64_t a, uint64_t b, uint64_t w) {
+__device__ __forceinline__ uint64_t dif_mul<Goldilocks>(uint64_t a, uint64_t b, uint64_t w, uint64_t) {
   return Goldilocks::mul(Goldilocks::sub(a, b), w);
 }
 
@@ -310,7 +360,7 @@ __device__ __forceinline__ void dif_reg(typename F::T (&x)[1 << LR], const Small
       if constexpr (j == 0)
         x[g + j + h] = F::sub(a, c);
       else
-        x[g + j + h] = dif_mul<F>(a, c, st.w[j << (5 - s)]);
+        x[g + j + h] = dif_mul<F>(a, c, st.w[j << (5 - s)], st.q[j << (5 - s)]);
     });
   });
 }
@@ -337,8 +387,8 @@ __global__ void __launch_bounds__(C << LR2)
   // Twiddles shared by the C columns of the CTA, staged once:
   //   tw_in[i*R1 + t]  = w_{2^K}^{i * rev(t)}   (phase-A twist of output t of thread i)
   //   tw_out[f]        = w_{2^hi}^{i_low * f}  (pass twist), or the 1/n scale on the last pass
-  T *tw_in = sm + S * R1;
-  T *tw_out = tw_in + (1 << K);
+  TwS<F> *tw_in = reinterpret_cast<TwS<F> *>(sm + S * R1);
+  TwS<F> *tw_out = tw_in + (1 << K);
 
   const uint32_t cta = blockIdx.x;
   const uint32_t chunk = cta % g.chunks_per_row;
@@ -354,11 +404,11 @@ __global__ void __launch_bounds__(C << LR2)
 
   for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) {
     const uint32_t ii = e / R1, tt = e % R1;
-    tw_in[e] = tw[(ii * (__brev(tt) >> (32 - LR1))) << (g.L - K)];
+    tw_in[e] = tw_stage<F>(tw[(ii * (__brev(tt) >> (32 - LR1))) << (g.L - K)]);
     if (g.twist)
-      tw_out[e] = tw[(i_low * e) << (g.L - hi)];  // i_low * e < 2^hi <= 2^L
+      tw_out[e] = tw_stage<F>(tw[(i_low * e) << (g.L - hi)]);  // i_low * e < 2^hi <= 2^L
     else if (post_scale)
-      tw_out[e] = post_scale;
+      tw_out[e] = tw_stage<F>(post_scale);
   }
 
   const size_t col0 = (size_t)blk * g.block_stride + (size_t)chunk * C + c;
@@ -376,11 +426,11 @@ __global__ void __launch_bounds__(C << LR2)
     }
     dif_reg<F, LR1>(x, st);
     __syncthreads();  // tw_in staged
-    const T *twi = tw_in + i * R1;
+    const TwS<F> *twi = tw_in + i * R1;
     sfor<R1>([&](auto tc) {
       constexpr int t = decltype(tc)::value;
       T v = x[t];
-      if constexpr (LR2 > 0 && t != 0) v = F::mul_tw(v, twi[t]);
+      if constexpr (LR2 > 0 && t != 0) v = tw_mul<F>(v, twi[t]);
       sm_a[rev_bits(t, LR1) * S] = v;
     });
   }
@@ -395,11 +445,11 @@ __global__ void __launch_bounds__(C << LR2)
     for (int ii = 0; ii < R2; ii++) y[ii] = sm_b[ii * C];
     dif_reg<F, LR2>(y, st);
     T *p = out + col0 + ((size_t)base_row * g.width) + (size_t)((__brev(f1) >> (32 - LR1)) * R2) * rs;
-    const T *two = tw_out + f1;
+    const TwS<F> *two = tw_out + f1;
     sfor<R2>([&](auto tc) {
       constexpr int t = decltype(tc)::value;
       T v = y[t];
-      if (scale_out) v = F::mul_tw(v, two[R1 * rev_bits(t, LR2)]);
+      if (scale_out) v = tw_mul<F>(v, two[R1 * rev_bits(t, LR2)]);
       *p = v;
       p += rs;
     });
@@ -442,7 +492,11 @@ static SmallTw<F> small_twiddles(bool inverse) {
   typename F::T w = two_adic_generator<F>(6), acc = 1;
   if (inverse) w = inv_host<F>(w);
   for (int e = 0; e < 32; e++) {
-    st.w[e] = Dom<F>::encode(acc);
+    st.w[e] = acc;
+    if constexpr (sizeof(typename F::T) == 4)
+      st.q[e] = BabyBear::shoup_quotient(acc);
+    else
+      st.q[e] = 0;
     acc = F::mul_host(acc, w);
   }
   return st;
@@ -454,7 +508,8 @@ static int launch_pass_c(const typename F::T *src, typename F::T *out, const Pas
                          cudaStream_t s) {
   using T = typename F::T;
   constexpr unsigned threads = C << LR2;
-  const size_t smem = ((size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) + (2u << (LR1 + LR2))) * sizeof(T);
+  const size_t smem = (size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) * sizeof(T) +
+                      (size_t)(2u << (LR1 + LR2)) * sizeof(TwS<F>);
   ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<F, LR1, LR2, C>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   ZKB_LAUNCH("ntt_pass", s, ntt_pass_kernel<F, LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(src, out, g, tw, scale, st));
@@ -592,10 +647,10 @@ __global__ void __launch_bounds__(C << LR2)
   constexpr int S = PassSmem<LR2, C>::STRIDE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
-  T *itw_in = sm + S * R1;        // [i][t] inverse inner twist
-  T *ftw_in = itw_in + (1 << K);  // [i][t] forward inner twist
-  T *ftw_out = ftw_in + (1 << K); // w_{2^L}^{m_lo * f}
-  T *cf = ftw_out + (1 << K);     // coset factors of the current coset
+  TwS<F> *itw_in = reinterpret_cast<TwS<F> *>(sm + S * R1);  // [i][t] inverse inner twist
+  TwS<F> *ftw_in = itw_in + (1 << K);                        // [i][t] forward inner twist
+  TwS<F> *ftw_out = ftw_in + (1 << K);                       // w_{2^L}^{m_lo * f}
+  TwS<F> *cf = ftw_out + (1 << K);                           // coset factors of the current coset
 
   const uint32_t cta = blockIdx.x;
   const uint32_t chunk = cta % g.chunks_per_row;
@@ -608,9 +663,9 @@ __global__ void __launch_bounds__(C << LR2)
   for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) {
     const uint32_t ii = e / R1, tt = e % R1;
     const uint32_t ex = (ii * (__brev(tt) >> (32 - LR1))) << lm;
-    itw_in[e] = itw[ex];
-    ftw_in[e] = ftw[ex];
-    ftw_out[e] = ftw_t[((size_t)m_lo << K) + e];  // w^(m_lo * e), stored contiguously per m_lo
+    itw_in[e] = tw_stage<F>(itw[ex]);
+    ftw_in[e] = tw_stage<F>(ftw[ex]);
+    ftw_out[e] = tw_stage<F>(ftw_t[((size_t)m_lo << K) + e]);  // w^(m_lo * e), contiguous per m_lo
   }
 
   const size_t colc = (size_t)chunk * C + c;
@@ -628,11 +683,11 @@ __global__ void __launch_bounds__(C << LR2)
     }
     dif_reg<F, LR1>(x, ist);
     __syncthreads();
-    const T *twi = itw_in + i * R1;
+    const TwS<F> *twi = itw_in + i * R1;
     sfor<R1>([&](auto tc) {
       constexpr int t = decltype(tc)::value;
       T v = x[t];
-      if constexpr (LR2 > 0 && t != 0) v = F::mul_tw(v, twi[t]);
+      if constexpr (LR2 > 0 && t != 0) v = tw_mul<F>(v, twi[t]);
       sm_a[rev_bits(t, LR1) * S] = v;
     });
   }
@@ -655,18 +710,18 @@ __global__ void __launch_bounds__(C << LR2)
     __syncthreads();  // previous users of the tile and of cf are done
     // factors of m = m_lo + e * 2^lm, stored contiguously per (coset, m_lo)
     const T *ct = ctab_t + (uint64_t)jc * g.n + ((size_t)m_lo << K);
-    for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) cf[e] = ct[e];
+    for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) cf[e] = tw_stage<F>(ct[e]);
     __syncthreads();
     {
       T x[R1];
 #pragma unroll
-      for (int j = 0; j < R1; j++) x[j] = F::mul_tw(coef[j], cf[j * R2 + i]);
+      for (int j = 0; j < R1; j++) x[j] = tw_mul<F>(coef[j], cf[j * R2 + i]);
       dif_reg<F, LR1>(x, fst);
-      const T *twi = ftw_in + i * R1;
+      const TwS<F> *twi = ftw_in + i * R1;
       sfor<R1>([&](auto tc) {
         constexpr int t = decltype(tc)::value;
         T v = x[t];
-        if constexpr (LR2 > 0 && t != 0) v = F::mul_tw(v, twi[t]);
+        if constexpr (LR2 > 0 && t != 0) v = tw_mul<F>(v, twi[t]);
         sm_a[rev_bits(t, LR1) * S] = v;
       });
     }
@@ -682,11 +737,11 @@ __global__ void __launch_bounds__(C << LR2)
       for (int ii = 0; ii < R2; ii++) y[ii] = sm_b[ii * C];
       dif_reg<F, LR2>(y, fst);
       T *p = blk + (size_t)((__brev(f1) >> (32 - LR1)) * R2) * rs;
-      const T *two = ftw_out + f1;
+      const TwS<F> *two = ftw_out + f1;
       sfor<R2>([&](auto tc) {
         constexpr int t = decltype(tc)::value;
         T v = y[t];
-        if (lm > 0) v = F::mul_tw(v, two[R1 * rev_bits(t, LR2)]);
+        if (lm > 0) v = tw_mul<F>(v, two[R1 * rev_bits(t, LR2)]);
         *p = v;
         p += rs;
       });
@@ -700,7 +755,8 @@ static int launch_fused_c(const typename F::T *in, typename F::T *out, const Fus
                           const typename F::T *ftw_t, cudaStream_t s) {
   using T = typename F::T;
   constexpr unsigned threads = C << LR2;
-  const size_t smem = ((size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) + (4u << (LR1 + LR2))) * sizeof(T);
+  const size_t smem = (size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) * sizeof(T) +
+                      (size_t)(4u << (LR1 + LR2)) * sizeof(TwS<F>);
   ZKB_CHECK_CUDA(cudaFuncSetAttribute(lde_fused_kernel<F, LR1, LR2, C>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   const uint64_t ctas = (uint64_t)g.chunks_per_row * g.blocks;
