@@ -215,6 +215,14 @@ ZKB_API int zkb_mmcs_commit(const zkb_hasher *hasher, const zkb_matrix *mats, si
 /* Device form: matrices are device pointers that must outlive the tree. */
 ZKB_API int zkb_mmcs_commit_dev(const zkb_hasher *hasher, const zkb_matrix *d_mats, size_t n_mats,
                         void *root_out, zkb_tree **tree_out, void *stream);
+/* Mmcs::commit of one device matrix (BabyBear, width-16 hasher) that also writes the
+ * alpha-reduction of every row, d_codeword[i] = sum_j alpha^j * mat[i][j] over the quartic
+ * extension (4 u32 per row, 16-byte aligned), in the same pass as the leaf hash — the
+ * reduction zkb_combine_columns_babybear_ext4_dev computes separately.  For a caller that
+ * knows alpha before the commitment (seeded challenges), e.g. one rank's row block of a
+ * commitment split over GPUs. */
+ZKB_API int zkb_mmcs_commit_reduce_dev(const zkb_hasher *hasher, const zkb_matrix *d_mat, const uint32_t *alpha,
+                                       void *root_out, zkb_tree **tree_out, uint32_t *d_codeword, void *stream);
 /* Digest layers (MerkleTree::digest_layers, merkle_tree.rs:40-54). */
 ZKB_API int zkb_tree_num_layers(const zkb_tree *tree);
 ZKB_API int64_t zkb_tree_layer_len(const zkb_tree *tree, int layer);

@@ -166,3 +166,22 @@ def test_one_rank_without_a_process_group():
     row, sibs = res.open(77)
     rows_ref, sibs_ref = pcs.mmcs.open_batch(77, tree)
     assert np.array_equal(row, rows_ref[0]) and all(np.array_equal(a, b) for a, b in zip(sibs, sibs_ref))
+
+
+@pytest.mark.parametrize("rows,width", [(1 << 10, 24), (1 << 9, 13), (1, 8), (1 << 8, 256)])
+def test_commit_reduce_equals_commit_then_combine(rows, width):
+    """zkb_mmcs_commit_reduce_dev: the same tree as zkb_mmcs_commit_dev and the same
+    codeword as zkb_combine_columns_babybear_ext4_dev, in one pass."""
+    m = torch.from_numpy(_trace(BB, max(rows.bit_length() - 1, 0), width, 9)[:rows].view(np.int32)).cuda()
+    alpha = np.array([11, 22, 33, 44], np.uint32)
+    mmcs = A.CudaMerkleTreeMmcs(BB, 42)
+    root_ref, tree_ref = mmcs.commit_dev([m])
+    cw_ref = torch.empty((rows, 4), dtype=torch.int32, device="cuda")
+    A.combine_columns_dev(m, alpha, cw_ref)
+    cw = torch.zeros((rows, 4), dtype=torch.int32, device="cuda")
+    root, tree = mmcs.commit_reduce_dev(m, alpha, cw)
+    assert np.array_equal(root, root_ref)
+    assert torch.equal(cw, cw_ref)
+    for i in sorted({0, rows // 2, rows - 1}):
+        a, b = mmcs.open_batch(i, tree), mmcs.open_batch(i, tree_ref)
+        assert np.array_equal(a[0][0], b[0][0]) and all(np.array_equal(x, y) for x, y in zip(a[1], b[1]))

@@ -188,6 +188,7 @@ SIGNATURES = {
     "zkb_challenger_free": (None, [_P]),
     "zkb_fri_commit_babybear_ext4_challenger_dev": (_I, [_P, _P, _P, _P, _P, _P]),
     "zkb_mmcs_compress": (_I, [_P, _P, _P, _SZ, _P]),
+    "zkb_mmcs_commit_reduce_dev": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "zkb_batch_create": (_I, [_P, _P, _SZ, _P, _P]),
     "zkb_batch_trace_ptr": (_I, [_P, _SZ, _P]),
     "zkb_batch_copy_in": (_I, [_P, _SZ, _P, _I, _P]),

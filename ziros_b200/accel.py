@@ -263,6 +263,24 @@ class CudaMerkleTreeMmcs:
         N.check(rc)
         return True
 
+    def commit_reduce_dev(self, mat, alpha, codeword) -> Tuple[np.ndarray, Tree]:
+        """Commit one CUDA int32 matrix (BabyBear, width-16 hasher) and write its rows'
+        alpha-reduction into `codeword` (rows x 4 int32 CUDA tensor) in the same pass."""
+        import torch
+
+        if codeword.shape != (mat.shape[0], 4):
+            raise ValueError("codeword must be rows x 4")
+        desc = N.Matrix(mat.data_ptr(), mat.shape[0], mat.shape[1])
+        a = np.ascontiguousarray(alpha, dtype=np.uint32)
+        root = np.zeros(self.digest_elems, dtype=dtype_of(self.field))
+        handle = C.c_void_p()
+        stream = C.c_void_p(torch.cuda.current_stream(mat.device).cuda_stream)
+        N.check(N.load().zkb_mmcs_commit_reduce_dev(C.byref(self.hasher), C.byref(desc), _ptr(a), _ptr(root),
+                                                    C.byref(handle), C.c_void_p(codeword.data_ptr()), stream))
+        t = Tree(handle, self.field, [tuple(mat.shape)])
+        t._keepalive = [mat]
+        return root, t
+
     def compress(self, left, right) -> np.ndarray:
         """TruncatedPermutation of digest pairs (host): left, right (n, OUT) -> (n, OUT)."""
         dt = dtype_of(self.field)

@@ -335,6 +335,27 @@ int zkb_mmcs_commit_dev(const zkb_hasher *hasher, const zkb_matrix *d_mats, size
   return tree_from(tree_out, tree, root_out, s);
 }
 
+int zkb_mmcs_commit_reduce_dev(const zkb_hasher *hasher, const zkb_matrix *d_mat, const uint32_t *alpha,
+                               void *root_out, zkb_tree **tree_out, uint32_t *d_codeword, void *stream) {
+  ZKB_ENTRY();
+  HasherSpec spec;
+  ZKB_TRY(hasher_spec(hasher, &spec));
+  ZKB_REQUIRE(spec.field == FIELD_BABYBEAR && spec.width == 16,
+              "the fused alpha-reduction runs with the BabyBear width-16 hasher");
+  ZKB_REQUIRE(d_mat != nullptr && d_mat->data != nullptr && d_mat->height > 0 && d_mat->width > 0 &&
+                  alpha != nullptr && d_codeword != nullptr,
+              "null or empty arguments");
+  ZKB_REQUIRE(((uintptr_t)d_codeword & 15) == 0, "codeword must be 16-byte aligned");
+  cudaStream_t s = resolve_stream(stream);
+  std::vector<TreeMatrix> mats{{d_mat->data, d_mat->height, d_mat->width}};
+  auto tree = std::make_unique<zkb_tree>();
+  ScratchBuf apow;
+  ZKB_TRY(alpha_powers_dev(alpha, (uint32_t)d_mat->width, &apow, s));
+  const LeafCombine comb{apow.as<uint4>(), (uint4 *)d_codeword};
+  ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s, false, &comb));
+  return tree_from(tree_out, tree, root_out, s);
+}
+
 int zkb_mmcs_commit(const zkb_hasher *hasher, const zkb_matrix *mats, size_t n_mats, void *root_out,
                     zkb_tree **tree_out) {
   ZKB_ENTRY();

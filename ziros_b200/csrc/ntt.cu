@@ -107,6 +107,18 @@ static int table_build_allowed(cudaStream_t s) {
   return ZKB_OK;
 }
 
+// Table memory lives as long as the process and is allocated outside the stream-ordered
+// pool, so permanent blocks do not fragment the pool that jobs allocate from and free to.
+static int table_alloc(void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    set_error("NTT table allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? ZKB_ERR_OOM : ZKB_ERR_CUDA;
+  }
+  return ZKB_OK;
+}
+
 // Publishes a table whose build was just enqueued on s.
 static int table_publish(DeviceTable &t, cudaStream_t s) {
   ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming));
@@ -134,14 +146,14 @@ int get_twiddles(int log_n, bool inverse, const typename F::T **out, cudaStream_
   ZKB_TRY(table_build_allowed(s));
   uint64_t n = 1ull << log_n;
   void *p = nullptr;
-  ZKB_TRY(dev_alloc(&p, n * sizeof(T), s));
+  ZKB_TRY(table_alloc(&p, n * sizeof(T)));
   T w = two_adic_generator<F>(log_n);
   if (inverse) w = inv_host<F>(w);
   DeviceTable t{p, n * sizeof(T)};
   int rc = launch_powers<F>((T *)p, n, w, 1, s);
   if (rc == ZKB_OK) rc = table_publish(t, s);
   if (rc != ZKB_OK) {
-    cudaFreeAsync(p, s);
+    cudaFree(p);  // error path only
     return rc;
   }
   ctx->twiddles[key] = t;
@@ -167,7 +179,7 @@ static int get_coset_table(int log_n, int log_b, typename F::T shift, const type
   ZKB_TRY(table_build_allowed(s));
   uint64_t n = 1ull << log_n, b = 1ull << log_b;
   void *p = nullptr;
-  ZKB_TRY(dev_alloc(&p, n * b * sizeof(T), s));
+  ZKB_TRY(table_alloc(&p, n * b * sizeof(T)));
   T w_bn = two_adic_generator<F>(log_n + log_b);
   T n_inv = inv_host<F>((T)(n % (uint64_t)F::P));
   T wj = 1;
@@ -179,7 +191,7 @@ static int get_coset_table(int log_n, int log_b, typename F::T shift, const type
   DeviceTable t{p, n * b * sizeof(T)};
   if (rc == ZKB_OK) rc = table_publish(t, s);
   if (rc != ZKB_OK) {
-    cudaFreeAsync(p, s);
+    cudaFree(p);  // error path only
     return rc;
   }
   ctx->cosets[key] = t;
@@ -223,7 +235,7 @@ static int get_fused_tables(int log_n, int log_b, typename F::T shift, int K, co
     // wait for their builds
     ZKB_TRY(table_build_allowed(s));
     void *p = nullptr;
-    ZKB_TRY(dev_alloc(&p, ((n << log_b) + n) * sizeof(T), s));
+    ZKB_TRY(table_alloc(&p, ((n << log_b) + n) * sizeof(T)));
     T *ct = (T *)p, *ft = ct + (n << log_b);
     ZKB_LAUNCH("table_fused", s, fused_tables_kernel<F><<<grid_for((n << log_b) + n, 256), 256, 0, s>>>(ctab, ftw, log_n, K, log_b, ct, ft));
     DeviceTable t{p, ((n << log_b) + n) * sizeof(T)};

@@ -92,6 +92,14 @@ class CudaShardOps:
     def commit(self, block: torch.Tensor):
         return self.mmcs.commit_dev([block])
 
+    def commit_reduce(self, block: torch.Tensor, alpha):
+        """The block's subtree and its rows' alpha-reduction in one pass (BabyBear, width 16)."""
+        if self.field != BABYBEAR or self.digest_elems != 8:
+            return None
+        seg = self.empty(block.shape[0], 4, ext4=True)
+        root, tree = self.mmcs.commit_reduce_dev(block, alpha, seg)
+        return root, tree, seg
+
     def open(self, tree, index: int) -> Tuple[np.ndarray, List[np.ndarray]]:
         rows, sibs = self.mmcs.open_batch(index, tree)
         return rows[0], sibs
@@ -237,8 +245,16 @@ def commit_sharded(cols: torch.Tensor, width: int, ops, group=None,
                 block[:, a:b].copy_(recv[off:off + m * w].view(m, w))
             off += m * w
         del recv
-    # 4. this rank's subtree
-    sub_root, tree = ops.commit(block)
+    # 4. this rank's subtree (with seeded FRI, alpha is known now: the leaf hash also
+    # reduces the rows)
+    seg = None
+    fused = None
+    if fri is not None and not fri.transcript and fri.alpha is not None and hasattr(ops, "commit_reduce"):
+        fused = ops.commit_reduce(block, np.ascontiguousarray(fri.alpha, dtype=np.uint32))
+    if fused is not None:
+        sub_root, tree, seg = fused
+    else:
+        sub_root, tree = ops.commit(block)
     # 5. the subtree roots, then the top levels
     d = ops.digest_elems
     roots_t = _all_gather(torch.as_tensor(np.asarray(sub_root).view(np.int32 if ops.dtype == torch.int32
@@ -265,7 +281,8 @@ def commit_sharded(cols: torch.Tensor, width: int, ops, group=None,
         if fri.alpha is None:
             raise ValueError("seeded FRI needs alpha")
         alpha = np.ascontiguousarray(fri.alpha, dtype=np.uint32)
-    seg = ops.combine(block, alpha)
+    if seg is None:
+        seg = ops.combine(block, alpha)
     codeword = _all_gather(seg, group)
     res.fri = ops.fri(codeword, fri, ch)
     res.alpha = alpha
