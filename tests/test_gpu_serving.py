@@ -172,3 +172,39 @@ def test_smallest_first_with_bounded_bypass():
 def test_unknown_policy_is_rejected():
     with pytest.raises(ValueError):
         Z.CommitEngine(slots=1, policy="lifo")
+
+
+def test_fifo_backfill_passes_a_waiting_job_a_bounded_number_of_times():
+    """FIFO with a budget that holds the big job and one small one but not the medium one:
+    small jobs backfill past the waiting medium job at most ZKB_ADMIT_MAX_BYPASS times."""
+    import time
+
+    from ziros_b200 import _native as N
+
+    MiB = 1 << 20
+    est = lambda log_h, w: (1 << log_h) * w * 4 + (2 << log_h) * w * 4 + 2 * (2 << log_h) * 64 + 64 * MiB
+    big_shape, med_shape, small_shape = (20, 64), (16, 32), (10, 8)
+    budget = est(*big_shape) + est(*small_shape) + 8 * MiB
+    assert est(*big_shape) + est(*med_shape) > budget
+    big = rand_field(0, (1 << big_shape[0], big_shape[1]), 80)
+    medium = rand_field(0, (1 << med_shape[0], med_shape[1]), 81)
+    smalls = [rand_field(0, (1 << small_shape[0], small_shape[1]), 82 + k) for k in range(N.ADMIT_MAX_BYPASS + 3)]
+    eng = Z.CommitEngine(slots=2, hbm_budget=budget, policy="fifo")
+    subs = []
+    for label, t in [("big", big), ("medium", medium)] + [(f"small{k}", s) for k, s in enumerate(smalls)]:
+        jid = eng.submit(t, field=0, seed=42, log_blowup=1)
+        subs.append((label, jid, time.perf_counter()))
+        if label == "big":
+            t0 = time.perf_counter()
+            while eng.stats()["queued"] and time.perf_counter() - t0 < 10:
+                time.sleep(0.0002)
+    starts = []
+    for label, jid, t_sub in subs:
+        res = eng.wait(jid)
+        starts.append((t_sub + res[2]["queue_ms"] / 1e3, label))
+    st = eng.stats()
+    eng.close()
+    order = [label for _, label in sorted(starts)]
+    assert order[0] == "big"
+    assert order.index("medium") <= 1 + N.ADMIT_MAX_BYPASS
+    assert st["hbm_peak"] <= budget

@@ -387,7 +387,7 @@ namespace {
 int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_trace, uint32_t log_h,
                     uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out,
                     cudaStream_t s, const uint32_t *alpha = nullptr, const zkb_fri_params *fri = nullptr,
-                    FriProof *fri_out = nullptr, std::mutex *upload_mu = nullptr) {
+                    FriProof *fri_out = nullptr, FairMutex *upload_mu = nullptr) {
   ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
   const size_t es = field_elem_bytes(spec.field);
   const uint64_t n = 1ull << log_h, N = n << log_blowup;
@@ -405,7 +405,7 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
       const size_t total = n * width * es, piece = 256ull << 20;
       for (size_t off = 0; off < total; off += piece) {
         const size_t len = total - off < piece ? total - off : piece;
-        std::lock_guard<std::mutex> lk(*upload_mu);
+        std::lock_guard<FairMutex> lk(*upload_mu);
         ZKB_CHECK_CUDA(cudaMemcpyAsync((char *)staged.p + off, (const char *)h_trace + off, len,
                                        cudaMemcpyHostToDevice, s));
         ZKB_TRY(wait_stream(s));
@@ -484,7 +484,7 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
 // before returning.
 int zkb::pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                      uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
-                     FriProof *fri_out, cudaStream_t s, std::mutex *upload_mu) {
+                     FriProof *fri_out, cudaStream_t s, FairMutex *upload_mu) {
   int rc = pcs_commit_impl(spec, nullptr, h_trace, log_h, width, log_blowup, root_out, nullptr, s,
                            alpha, fri, fri_out, upload_mu);
   if (fri_out) fri_out->release_device();

@@ -1,7 +1,9 @@
 // engine.cuh — internal host-side interfaces between the CUDA modules.
 #pragma once
 #include <array>
+#include <condition_variable>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -128,11 +130,36 @@ struct FriProof {
   ~FriProof();
 };
 
+// First-come first-served lock (tickets): a thread that releases it and asks again goes
+// behind the threads already waiting, so a job copying many pieces in a loop lets a
+// waiting job's piece through between two of its own.  BasicLockable.
+class FairMutex {
+ public:
+  void lock() {
+    std::unique_lock<std::mutex> lk(mu_);
+    const uint64_t t = next_++;
+    cv_.wait(lk, [&] { return serving_ == t; });
+  }
+  void unlock() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      serving_++;
+    }
+    cv_.notify_all();
+  }
+
+ private:
+  std::mutex mu_;
+  std::condition_variable cv_;
+  uint64_t next_ = 0, serving_ = 0;
+};
+
 // One PCS commit job from host memory (+ FRI when `fri` is set), device state released.
-// upload_mu (may be NULL) serialises the host-to-device copies of concurrent jobs.
+// upload_mu (may be NULL) serialises the host-to-device copies of concurrent jobs, taken
+// per piece of the trace.
 int pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                 uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
-                FriProof *fri_out, cudaStream_t s, std::mutex *upload_mu = nullptr);
+                FriProof *fri_out, cudaStream_t s, FairMutex *upload_mu = nullptr);
 int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
                              const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s);
 // With `ch` set, every round's root is observed before its beta is sampled, the final

@@ -249,7 +249,11 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
   MatList ml;
   ZKB_TRY(make_list(0, ng, &ml));
   const unsigned thr = 128;
-  const unsigned cap = (unsigned)ctx->sm_count * 16u;
+  // One row (or pair) per thread and as many blocks as that takes: blocks retire every few
+  // milliseconds, so kernels of other streams (other jobs of the engine, which gives small
+  // jobs higher stream priority) get SMs in between instead of waiting for the whole grid.
+  const unsigned cap = 1u << 30;
+  (void)ctx;
   if constexpr (std::is_same<F, BabyBear>::value && W == 16) {
     if (comb) {
       ZKB_REQUIRE(nm == 1, "the fused alpha-reduction takes one matrix");

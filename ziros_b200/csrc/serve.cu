@@ -2,9 +2,10 @@
 //
 // Jobs (a host trace to commit, optionally followed by the FRI commit phase on the
 // alpha-reduced LDE) are submitted without blocking.  `slots` worker threads each
-// own a CUDA stream; a worker admits a queued job whose device-memory estimate fits
-// what is left of the HBM budget (the oldest such job, or with ZKB_ADMIT_SMALLEST the
-// one with the fewest cells, under a bound on how often a job is passed over), copies the trace
+// own CUDA streams (one per job-size class, small jobs at the highest priority); a worker
+// admits a queued job whose device-memory estimate fits what is left of the HBM budget
+// (the one with the fewest cells, or with ZKB_ADMIT_FIFO the oldest, under a bound on how
+// often a job is passed over), copies the trace
 // in on its stream, keeps the LDE, the trees and the FRI layers device-resident until
 // the job's answers are on the host, then releases the memory and wakes the queue.
 // Jobs on different workers overlap on the GPU (one job's copy under another's
@@ -97,9 +98,9 @@ uint64_t job_bytes(const zkb_job_desc &d) {
 struct zkb_engine {
   int device = 0;
   uint64_t budget = 0, in_use = 0;
-  uint32_t policy = ZKB_ADMIT_FIFO;
+  uint32_t policy = ZKB_ADMIT_SMALLEST;
   std::mutex mu;
-  std::mutex upload_mu;  // one job's trace crosses PCIe at a time
+  FairMutex upload_mu;  // one job's trace piece crosses PCIe at a time, pieces in request order
   std::condition_variable cv_queue, cv_done;
   std::deque<std::shared_ptr<Job>> queue;
   std::map<uint64_t, std::shared_ptr<Job>> jobs;
@@ -114,9 +115,13 @@ struct zkb_engine {
   std::deque<std::shared_ptr<Job>>::iterator pick() {
     auto fits = [&](const std::shared_ptr<Job> &j) { return in_use + j->mem_estimate <= budget; };
     if (policy != ZKB_ADMIT_SMALLEST) {
-      auto it = queue.begin();
-      while (it != queue.end() && !fits(*it)) ++it;
-      return it;
+      // the oldest fitting job; a job that younger ones have passed ZKB_ADMIT_MAX_BYPASS
+      // times is admitted next, and nothing passes it while it waits for memory
+      for (auto it = queue.begin(); it != queue.end(); ++it) {
+        if (fits(*it)) return it;
+        if ((*it)->bypassed >= ZKB_ADMIT_MAX_BYPASS) return queue.end();
+      }
+      return queue.end();
     }
     auto best = queue.end();
     for (auto it = queue.begin(); it != queue.end(); ++it) {
@@ -126,10 +131,24 @@ struct zkb_engine {
     return best;
   }
 
+  // Stream priority by job size: small jobs' kernels are scheduled ahead of large jobs'
+  // as blocks retire, so a small job does not wait behind a large job's whole kernel.
+  static int size_class(const Job &j) {
+    const uint64_t c = cells(j);
+    return c < (1ull << 26) ? 0 : c < (1ull << 30) ? 1 : 2;
+  }
+
   void worker_loop() {
     cudaSetDevice(device);
-    cudaStream_t s;
-    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return;
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    const int prio[3] = {greatest, (least + greatest) / 2, least};
+    cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
+    for (int k = 0; k < 3; k++)
+      if (cudaStreamCreateWithPriority(&streams[k], cudaStreamNonBlocking, prio[k]) != cudaSuccess) {
+        for (int q = 0; q < k; q++) cudaStreamDestroy(streams[q]);
+        return;
+      }
     for (;;) {
       std::shared_ptr<Job> job;
       {
@@ -157,6 +176,7 @@ struct zkb_engine {
       std::unique_ptr<zkb_fri_proof> fri;
       if (job->desc.with_fri) fri = std::make_unique<zkb_fri_proof>();
       zkb_fri_params prm = job->desc.fri;
+      cudaStream_t s = streams[size_class(*job)];
       int rc = pcs_job_run(job->spec, job->desc.trace, job->desc.log_h, job->desc.width,
                            job->desc.log_blowup, job->desc.alpha, job->desc.with_fri ? &prm : nullptr,
                            job->root, fri ? &fri->f : nullptr, s, &upload_mu);
@@ -175,7 +195,7 @@ struct zkb_engine {
       cv_queue.notify_all();
       cv_done.notify_all();
     }
-    cudaStreamDestroy(s);
+    for (cudaStream_t q : streams) cudaStreamDestroy(q);
   }
 };
 
