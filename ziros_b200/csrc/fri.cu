@@ -193,9 +193,7 @@ static int fold_params(const uint32_t beta[4], Ext4Params *prm) {
 static int fri_fold_hash_dev(const uint32_t *cw_in, uint32_t *cw_out, int log_out, const uint32_t *beta,
                              uint32_t *leaf_digests, const P2Params<BabyBear, 16> &p, cudaStream_t s) {
   const uint64_t n_leaves = 1ull << (log_out - 1);
-  DeviceContext *ctx;
-  ZKB_TRY(current_context(&ctx));
-  const unsigned grid = grid_for(n_leaves, 128, (unsigned)ctx->sm_count * 16u);
+  const unsigned grid = grid_for(n_leaves, 128, 1u << 30);  // one leaf per thread
   if (beta) {
     Ext4Params prm;
     ZKB_TRY(fold_params(beta, &prm));

@@ -206,10 +206,13 @@ int launch_trees(const Tables &t, const LeafJob *d_leaf, const CompJob *d_comp, 
   DeviceContext *ctx;
   ZKB_TRY(current_context(&ctx));
   const int n = (int)t.leaf.size();
+  // one row (or compression) per thread: short-lived blocks, so concurrent streams
+  // interleave at block granularity
+  (void)ctx;
   if (leaf_name)
-    ZKB_LAUNCH(leaf_name, s, mt_leaf_kernel<F, W><<<grid_for(t.total_rows, leaf_threads, (unsigned)ctx->sm_count * (2048u / leaf_threads)), leaf_threads, n * sizeof(uint64_t), s>>>(d_leaf, n, t.total_rows, p));
+    ZKB_LAUNCH(leaf_name, s, mt_leaf_kernel<F, W><<<grid_for(t.total_rows, leaf_threads, 1u << 30), leaf_threads, n * sizeof(uint64_t), s>>>(d_leaf, n, t.total_rows, p));
   for (size_t l = 0; l < t.lvl_cnt.size(); l++) {
-    ZKB_LAUNCH(comp_name, s, mt_compress_kernel<F, W><<<grid_for(t.lvl_total[l], 128, (unsigned)ctx->sm_count * 16u), 128, t.lvl_cnt[l] * sizeof(uint64_t), s>>>(d_comp + t.lvl_off[l], (int)t.lvl_cnt[l], t.lvl_total[l], p));
+    ZKB_LAUNCH(comp_name, s, mt_compress_kernel<F, W><<<grid_for(t.lvl_total[l], 128, 1u << 30), 128, t.lvl_cnt[l] * sizeof(uint64_t), s>>>(d_comp + t.lvl_off[l], (int)t.lvl_cnt[l], t.lvl_total[l], p));
   }
   ZKB_LAUNCH(root_name, s, mt_roots_kernel<T, OUT><<<(n * OUT + 127) / 128, 128, 0, s>>>(d_root_off, (const T *)base, n, (T *)d_roots));
   return ZKB_OK;
