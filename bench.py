@@ -816,15 +816,15 @@ def run_serving(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     # service time of the plain path: the calibration list back to back on one slot
     calib = serving_jobs(wl, wl["jobs"], wl["seed"])
     eng1 = Z.CommitEngine(slots=1, policy="fifo")
-    engN = Z.CommitEngine(slots=wl["slots"])  # the engine's default admission: fewest cells first
-    engF = Z.CommitEngine(slots=wl["slots"], policy="fifo")
+    engN = Z.CommitEngine(slots=wl["slots"])  # the engine's default admission: oldest fitting job first
+    engS = Z.CommitEngine(slots=wl["slots"], policy="smallest")
     drive(eng1, calib[:4], 0, 1)  # warm-up: tables, memory pool
     _, span = drive(eng1, calib, 0, 2)
     service_s = span / len(calib)
     mu = 1.0 / service_s
     rates = [0.5 * mu, 0.8 * mu, 1.0 * mu, 1.5 * mu]
     drive(engN, calib[:4], 0, 3)
-    drive(engF, calib[:4], 0, 4)
+    drive(engS, calib[:4], 0, 4)
     sweep = []
     h2d = 0
     sampler = ClockSampler(local_rank)
@@ -832,19 +832,19 @@ def run_serving(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     for k, rate in enumerate(rates):
         jobs = serving_jobs(wl, wl["jobs"], wl["seed"] + 100 + k)
         r_b, s_b = drive(engN, jobs, rate, 1000 + k)
-        r_s, s_s = drive(engF, jobs, rate, 1000 + k)
+        r_s, s_s = drive(engS, jobs, rate, 1000 + k)
         r_p, s_p = drive(eng1, jobs, rate, 1000 + k)
         for a, b, c in zip(r_b, r_p, r_s):
             assert (a[0] == b[0]).all() and (a[1].roots == b[1].roots).all(), "a result differs in the mix"
             assert (c[0] == b[0]).all() and (c[1].roots == b[1].roots).all(), "a result differs in the mix"
         sweep.append({"rate_jobs_per_s": rate, "load": rate / mu, "batched": summarize(jobs, r_b, s_b),
-                      "batched_fifo": summarize(jobs, r_s, s_s), "plain": summarize(jobs, r_p, s_p)})
+                      "batched_smallest": summarize(jobs, r_s, s_s), "plain": summarize(jobs, r_p, s_p)})
         h2d = 4 * sum(h * w for h, w in jobs)
     clocks = sampler.stop()
     st = engN.stats()
     eng1.close()
     engN.close()
-    engF.close()
+    engS.close()
     top = sweep[-1]
     line = {
         "metric": METRIC, "value": top["batched"]["cells_per_s"], "unit": "cells/s", "n_gpus": 1,
@@ -858,11 +858,11 @@ def run_serving(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
                    "pinned_host_gb": hmax * 4 / 1e9, "service_ms_plain": 1e3 * service_s,
                    "l2": "inputs larger than L2"},
         "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"],
-        "policies": {"batched": f"{wl['slots']} slots, fewest cells first (the engine default), a job passed "
-                                f"over {N.ADMIT_MAX_BYPASS} times goes next",
-                     "batched_fifo": f"{wl['slots']} slots, oldest fitting job first, same bypass bound",
+        "policies": {"batched": f"{wl['slots']} slots, oldest fitting job first (the engine default), a job "
+                                f"passed over {N.ADMIT_MAX_BYPASS} times goes next",
+                     "batched_smallest": f"{wl['slots']} slots, fewest cells first, same bypass bound",
                      "plain": "1 slot, FIFO"},
-        "batched_fifo": top["batched_fifo"],
+        "batched_smallest": top["batched_smallest"],
         "plain": top["plain"],
         "sweep": sweep,
         "e2e": {"value": top["batched"]["cells_per_s"], "unit": "cells/s", "h2d_bytes_per_step": h2d,

@@ -446,17 +446,17 @@ ZKB_API void zkb_rt_free(zkb_rt *rt);
 typedef struct {
   uint32_t slots;        /* concurrent jobs */
   uint64_t hbm_budget;   /* bytes for job state; 0 = free device memory minus 2 GiB */
-  uint32_t policy;       /* admission: ZKB_ADMIT_SMALLEST (0, the default) or ZKB_ADMIT_FIFO */
+  uint32_t policy;       /* admission: ZKB_ADMIT_FIFO (0, the default) or ZKB_ADMIT_SMALLEST */
 } zkb_engine_config;
-/* SMALLEST: the fitting job with the fewest trace cells.  FIFO: the oldest queued job that
- * fits the remaining budget (a job waiting for memory may be passed by younger jobs that
- * fit).  Under both, a job passed over ZKB_ADMIT_MAX_BYPASS times is admitted next, and
+/* FIFO: the oldest queued job that fits the remaining budget (a job waiting for memory may
+ * be passed by younger jobs that fit).  SMALLEST: the fitting job with the fewest trace
+ * cells.  Under both, a job passed over ZKB_ADMIT_MAX_BYPASS times is admitted next, and
  * while it does not fit nothing else is admitted (no job waits forever).  Whatever the
  * policy, a running job's stream priority follows its size (small jobs' kernels are
  * scheduled first as blocks retire) and trace uploads share the link piece by piece in
  * request order. */
-#define ZKB_ADMIT_SMALLEST 0
-#define ZKB_ADMIT_FIFO 1
+#define ZKB_ADMIT_FIFO 0
+#define ZKB_ADMIT_SMALLEST 1
 #define ZKB_ADMIT_MAX_BYPASS 8
 typedef struct {
   zkb_hasher hasher;

@@ -61,7 +61,7 @@ class EngineConfig(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("hbm_budget", C.c_uint64), ("policy", C.c_uint32)]
 
 
-ADMIT_SMALLEST, ADMIT_FIFO, ADMIT_MAX_BYPASS = 0, 1, 8
+ADMIT_FIFO, ADMIT_SMALLEST, ADMIT_MAX_BYPASS = 0, 1, 8
 
 
 class JobDesc(C.Structure):

@@ -537,8 +537,8 @@ class CommitEngine:
 
     POLICIES = {"fifo": N.ADMIT_FIFO, "smallest": N.ADMIT_SMALLEST}
 
-    def __init__(self, slots: int = 2, hbm_budget: int = 0, policy: str = "smallest"):
-        """policy "smallest" (default): fewest cells first; "fifo": oldest fitting job
+    def __init__(self, slots: int = 2, hbm_budget: int = 0, policy: str = "fifo"):
+        """policy "fifo" (default): oldest fitting job first; "smallest": fewest cells
         first.  Under both a job passed over ADMIT_MAX_BYPASS times goes next."""
         lib = N.load()
         self._h = C.c_void_p()

@@ -4,8 +4,8 @@
 // alpha-reduced LDE) are submitted without blocking.  `slots` worker threads each
 // own CUDA streams (one per job-size class, small jobs at the highest priority); a worker
 // admits a queued job whose device-memory estimate fits what is left of the HBM budget
-// (the one with the fewest cells, or with ZKB_ADMIT_FIFO the oldest, under a bound on how
-// often a job is passed over), copies the trace
+// (the oldest such job, or with ZKB_ADMIT_SMALLEST the one with the fewest cells, under a
+// bound on how often a job is passed over), copies the trace
 // in on its stream, keeps the LDE, the trees and the FRI layers device-resident until
 // the job's answers are on the host, then releases the memory and wakes the queue.
 // Jobs on different workers overlap on the GPU (one job's copy under another's
@@ -98,7 +98,7 @@ uint64_t job_bytes(const zkb_job_desc &d) {
 struct zkb_engine {
   int device = 0;
   uint64_t budget = 0, in_use = 0;
-  uint32_t policy = ZKB_ADMIT_SMALLEST;
+  uint32_t policy = ZKB_ADMIT_FIFO;
   std::mutex mu;
   FairMutex upload_mu;  // one job's trace piece crosses PCIe at a time, pieces in request order
   std::condition_variable cv_queue, cv_done;
