@@ -387,7 +387,8 @@ namespace {
 int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_trace, uint32_t log_h,
                     uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out,
                     cudaStream_t s, const uint32_t *alpha = nullptr, const zkb_fri_params *fri = nullptr,
-                    FriProof *fri_out = nullptr, FairMutex *upload_mu = nullptr) {
+                    FriProof *fri_out = nullptr, UploadGate *upload_mu = nullptr,
+                    std::unique_lock<std::mutex> *compute_lock = nullptr) {
   ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
   const size_t es = field_elem_bytes(spec.field);
   const uint64_t n = 1ull << log_h, N = n << log_blowup;
@@ -400,21 +401,31 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
     if (upload_mu) {
       // one upload at a time: concurrent jobs would split the PCIe link and all start
       // computing late; serialised, each upload runs under the other jobs' kernels.  The
-      // token is taken per 256 MiB piece, so a small job's upload waits for one piece of
-      // a large job's, not for all of it.
+      // link is taken per 256 MiB piece, the upload with the fewest bytes left first, so a
+      // small job's upload waits for one piece of a large job's, not for all of it.
       const size_t total = n * width * es, piece = 256ull << 20;
       for (size_t off = 0; off < total; off += piece) {
         const size_t len = total - off < piece ? total - off : piece;
-        std::lock_guard<FairMutex> lk(*upload_mu);
-        ZKB_CHECK_CUDA(cudaMemcpyAsync((char *)staged.p + off, (const char *)h_trace + off, len,
-                                       cudaMemcpyHostToDevice, s));
-        ZKB_TRY(wait_stream(s));
+        upload_mu->acquire(total - off);
+        int rc = ZKB_OK;
+        const cudaError_t e = cudaMemcpyAsync((char *)staged.p + off, (const char *)h_trace + off, len,
+                                              cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+          set_error("cudaMemcpyAsync of a trace piece failed: %s", cudaGetErrorString(e));
+          rc = ZKB_ERR_CUDA;
+        }
+        if (rc == ZKB_OK) rc = wait_stream(s);
+        upload_mu->release();
+        ZKB_TRY(rc);
       }
     } else {
       ZKB_CHECK_CUDA(cudaMemcpyAsync(staged.p, h_trace, n * width * es, cudaMemcpyHostToDevice, s));
     }
     d_trace = staged.p;
   }
+  // an engine job waits here, its trace on the device, until the jobs of its size class
+  // ahead of it have finished computing
+  if (compute_lock) compute_lock->lock();
   void *lde = nullptr;
   ZKB_TRY(dev_alloc(&lde, N * width * es, s));
   tree->t.owned.push_back(lde);
@@ -452,6 +463,12 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
   } else {
     ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));
   }
+  if (compute_lock && compute_lock->owns_lock()) {
+    // the large kernels (LDE, leaf hash, tree) are done when this returns; the FRI phase's
+    // small kernels and host round trips overlap the next job's LDE
+    ZKB_TRY(wait_stream(s));
+    compute_lock->unlock();
+  }
   if (fri) {
     // alpha-reduction of the committed columns (unless fused above), then the FRI commit phase
     const int log_n = (int)(log_h + log_blowup);
@@ -484,12 +501,14 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
 // before returning.
 int zkb::pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                      uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
-                     FriProof *fri_out, cudaStream_t s, FairMutex *upload_mu) {
+                     FriProof *fri_out, cudaStream_t s, UploadGate *upload_mu, std::mutex *compute_mu) {
+  std::unique_lock<std::mutex> cl;
+  if (compute_mu) cl = std::unique_lock<std::mutex>(*compute_mu, std::defer_lock);
   int rc = pcs_commit_impl(spec, nullptr, h_trace, log_h, width, log_blowup, root_out, nullptr, s,
-                           alpha, fri, fri_out, upload_mu);
+                           alpha, fri, fri_out, upload_mu, compute_mu ? &cl : nullptr);
   if (fri_out) fri_out->release_device();
   if (rc == ZKB_OK) ZKB_TRY(wait_stream(s));
-  return rc;
+  return rc;  // the compute lock (if taken) is released here, after the job's work
 }
 
 extern "C" {

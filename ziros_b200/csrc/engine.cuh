@@ -4,6 +4,7 @@
 #include <condition_variable>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <vector>
 
 #include "common.cuh"
@@ -130,20 +131,25 @@ struct FriProof {
   ~FriProof();
 };
 
-// First-come first-served lock (tickets): a thread that releases it and asks again goes
-// behind the threads already waiting, so a job copying many pieces in a loop lets a
-// waiting job's piece through between two of its own.  BasicLockable.
-class FairMutex {
+// The PCIe link of an engine, handed out one trace piece at a time.  Among the waiting
+// uploads the one with the fewest bytes left goes next (ties: the earlier request): an
+// upload in progress keeps the link against a later one of equal size, so equal jobs upload
+// one after another and the first starts computing early, while a small job's upload waits
+// for at most one piece of a large one.
+class UploadGate {
  public:
-  void lock() {
+  void acquire(uint64_t bytes_left) {
     std::unique_lock<std::mutex> lk(mu_);
-    const uint64_t t = next_++;
-    cv_.wait(lk, [&] { return serving_ == t; });
+    const std::pair<uint64_t, uint64_t> key{bytes_left, next_++};
+    waiting_.insert(key);
+    cv_.wait(lk, [&] { return !busy_ && *waiting_.begin() == key; });
+    waiting_.erase(waiting_.begin());
+    busy_ = true;
   }
-  void unlock() {
+  void release() {
     {
       std::lock_guard<std::mutex> lk(mu_);
-      serving_++;
+      busy_ = false;
     }
     cv_.notify_all();
   }
@@ -151,15 +157,20 @@ class FairMutex {
  private:
   std::mutex mu_;
   std::condition_variable cv_;
-  uint64_t next_ = 0, serving_ = 0;
+  std::set<std::pair<uint64_t, uint64_t>> waiting_;
+  uint64_t next_ = 0;
+  bool busy_ = false;
 };
 
 // One PCS commit job from host memory (+ FRI when `fri` is set), device state released.
 // upload_mu (may be NULL) serialises the host-to-device copies of concurrent jobs, taken
-// per piece of the trace.
+// per piece of the trace; compute_mu (may be NULL) is held from the end of the upload until
+// the job's tree is built, so jobs sharing it run their large kernels one at a time while
+// others upload (and their FRI phases overlap the next job's LDE).
 int pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                 uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
-                FriProof *fri_out, cudaStream_t s, FairMutex *upload_mu = nullptr);
+                FriProof *fri_out, cudaStream_t s, UploadGate *upload_mu = nullptr,
+                std::mutex *compute_mu = nullptr);
 int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
                              const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s);
 // With `ch` set, every round's root is observed before its beta is sampled, the final

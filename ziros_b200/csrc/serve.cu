@@ -100,7 +100,11 @@ struct zkb_engine {
   uint64_t budget = 0, in_use = 0;
   uint32_t policy = ZKB_ADMIT_FIFO;
   std::mutex mu;
-  FairMutex upload_mu;  // one job's trace piece crosses PCIe at a time, pieces in request order
+  UploadGate upload_mu;  // one trace piece crosses PCIe at a time, the fewest bytes left first
+  // One job of each size class runs its LDE and tree at a time: equal jobs pipeline one's
+  // upload under another's kernels instead of interleaving their kernels block by block;
+  // jobs of different classes still overlap, the smaller at the higher stream priority.
+  std::mutex compute_mu[3];
   std::condition_variable cv_queue, cv_done;
   std::deque<std::shared_ptr<Job>> queue;
   std::map<uint64_t, std::shared_ptr<Job>> jobs;
@@ -179,7 +183,8 @@ struct zkb_engine {
       cudaStream_t s = streams[size_class(*job)];
       int rc = pcs_job_run(job->spec, job->desc.trace, job->desc.log_h, job->desc.width,
                            job->desc.log_blowup, job->desc.alpha, job->desc.with_fri ? &prm : nullptr,
-                           job->root, fri ? &fri->f : nullptr, s, &upload_mu);
+                           job->root, fri ? &fri->f : nullptr, s, &upload_mu,
+                           &compute_mu[size_class(*job)]);
       std::string err = rc == ZKB_OK ? "" : zkb_last_error_message();
       ENGINE_TRACE("end job %llu rc=%d %s\n", (unsigned long long)job->id, rc, err.c_str());
       log_job(*job, rc, Clock::now());
