@@ -453,8 +453,8 @@ typedef struct {
  * cells.  Under both, a job passed over ZKB_ADMIT_MAX_BYPASS times is admitted next, and
  * while it does not fit nothing else is admitted (no job waits forever).  Whatever the
  * policy, a running job's stream priority follows its size (small jobs' kernels are
- * scheduled first as blocks retire) and trace uploads share the link piece by piece in
- * request order. */
+ * scheduled first as blocks retire), trace uploads take the link piece by piece with the
+ * fewest bytes left first, and one job per size class runs its LDE and tree at a time. */
 #define ZKB_ADMIT_FIFO 0
 #define ZKB_ADMIT_SMALLEST 1
 #define ZKB_ADMIT_MAX_BYPASS 8
