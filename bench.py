@@ -68,6 +68,31 @@ E2E_SLOTS = 4  # engine slots of the e2e leg: a job's H2D copy overlaps the othe
 METRIC = "trace cells/s committed (LDE+Poseidon2 Merkle+FRI), batched vs plain; p99 ms"
 
 
+def synthetic_trace(field: int, rows: int, width: int, seed: int, out=None):
+    """Seeded uniform field elements as a row-major (rows, width) numpy array, the same on
+    every machine: block k of 2^24 elements is numpy's exact bounded draw from
+    default_rng([seed, k]), so blocks fill in parallel.  `out` (a numpy view of, e.g., a
+    pinned buffer) receives the values in place."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    dt, p = (np.uint32, BB_P) if field == 0 else (np.uint64, GL_P)
+    n = rows * width
+    flat = np.empty(n, dt) if out is None else out.reshape(-1)
+    assert flat.dtype == dt and flat.size == n
+    block = 1 << 24
+
+    def fill(k):
+        off = k * block
+        m = min(block, n - off)
+        flat[off:off + m] = np.random.default_rng([seed, k]).integers(0, p, size=m, dtype=dt)
+
+    with ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
+        list(ex.map(fill, range((n + block - 1) // block)))
+    return flat.reshape(rows, width)
+
+
 def p2_field_muls(field: int, p2w: int) -> int:
     """Algorithmic field multiplications of one permutation: 4 per S-box (x^7) on
     R_F*W + R_P lanes, W per internal round for the diagonal."""
@@ -187,19 +212,24 @@ def run_reference(args, wl: dict, rank: int, world: int) -> int:
         times.append(dt)
     total = sum(times)
     value = cells * len(times) / total
-    sample = f"2^{log_rows} x {wl['width']} rows x cols of the {args.workload} workload per step"
+    fri_part = " + alpha-reduction + FRI commit phase and queries" if wl["field"] == 0 else ""
+    sample = (f"2^{log_rows} x {wl['width']} trace per step (LDE x2^{wl['log_blowup']} + MMCS{fri_part}) of the "
+              f"2^{wl['log_h']} x {wl['width']} {args.workload} job; value = cells of the sample / its time, "
+              f"a rate measured on the smaller height, not extrapolated")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32" if wl["field"] == 0 else "u64", "data": "synthetic (seeded uniform field elements)",
         "config": {"workload": args.workload, "log_rows": wl["log_h"], "width": wl["width"],
-                   "log_blowup": wl["log_blowup"], "poseidon2_width": wl["p2w"]},
+                   "log_blowup": wl["log_blowup"], "poseidon2_width": wl["p2w"], "sample_log_rows": log_rows},
         "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "reference CPU path restated in C (oracle/); the Rust/p3 build of the reference "
-                "cannot be compiled here (no Rust toolchain, p3 0.4.2 crates absent)",
+        "note": "reference CPU path restated in C (oracle/, OpenMP over all host cores) with scalar u64/u128 "
+                "remainder arithmetic per product, not p3's packed-SIMD Montgomery kernels, so it is slower "
+                "than the reference's own CPU build would be; that build cannot be compiled here (no Rust "
+                "toolchain, p3 0.4.2 crates absent)",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -296,6 +326,92 @@ def fill_pinned(torch, field: int, n: int, seed: int, device):
     return out
 
 
+def golden_check(workload: str, wl: dict, root, pf) -> dict:
+    """Compares the timed job's answers with the oracle's for the same seeded trace
+    (tests/golden/fullsize.json, written by tests/golden/make_fullsize.py); a mismatch
+    fails the run."""
+    import hashlib
+
+    import numpy as np
+
+    key = "goldilocks_2^20x64_b4" if workload.startswith("goldilocks_2^20x64_b4") else workload
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "fullsize.json")) as f:
+            g = json.load(f).get(key)
+    except (OSError, ValueError):
+        g = None
+    if g is None:
+        return {"checked": False, "why": "no oracle answers committed for this workload"}
+    if wl["field"] == 1:
+        want = g[f"root_w{wl['p2w']}"]
+        assert [str(int(x)) for x in root] == want, "root differs from the oracle's"
+        return {"checked": True, "compared": f"MMCS root (width-{wl['p2w']} Poseidon2) equal to the oracle's"}
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()  # noqa: E731
+    assert root.tolist() == g["root"], "root differs from the oracle's"
+    assert pf.roots.tolist() == g["fri_roots"] and pf.betas.tolist() == g["fri_betas"], "FRI roots differ"
+    assert pf.final.tolist() == g["fri_final"], "FRI final codeword differs"
+    assert pf.query_indices.tolist() == g["query_indices"], "query indices differ"
+    assert sha(pf.query_rows) == g["query_rows_sha256"], "query rows differ"
+    assert sha(pf.query_siblings) == g["query_siblings_sha256"], "query paths differ"
+    return {"checked": True, "compared": "trace root, every FRI root and beta, the final codeword and all "
+                                         "query rows and paths of the last timed step equal to the oracle's"}
+
+
+class GpuLocalMemory:
+    """Within the block, the process runs on the host CPUs attached to the GPU's PCIe root
+    (sysfs local_cpulist), so pinned pages first touched there sit in the GPU's NUMA node;
+    the previous CPU set comes back afterwards."""
+
+    def __init__(self, torch, device_index: int):
+        self.cpus = None
+        self.prev = None
+        try:
+            pr = torch.cuda.get_device_properties(device_index)
+            bdf = "%04x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            with open(f"/sys/bus/pci/devices/{bdf}/local_cpulist") as f:
+                cpus = set()
+                for part in f.read().strip().split(","):
+                    a, _, b = part.partition("-")
+                    cpus.update(range(int(a), int(b or a) + 1))
+            self.cpus = cpus & os.sched_getaffinity(0)
+        except (OSError, ValueError, AttributeError):
+            self.cpus = None
+
+    def __enter__(self):
+        if self.cpus:
+            self.prev = os.sched_getaffinity(0)
+            os.sched_setaffinity(0, self.cpus)
+        return self
+
+    def __exit__(self, *exc):
+        if self.prev:
+            os.sched_setaffinity(0, self.prev)
+
+    def describe(self) -> str:
+        return f"{len(self.cpus)} GPU-local host CPUs" if self.cpus else "GPU locality unknown (no sysfs entry)"
+
+
+def measure_h2d(torch, pinned, dev, reps: int = 3) -> float:
+    """Pinned host -> device copy bandwidth of the trace buffer on this box (GB/s, best of
+    `reps`): 256 MiB pieces, one cudaMemcpyAsync each, as the engine uploads a job."""
+    flat = pinned.view(-1)
+    dst = torch.empty_like(flat, device=dev)
+    piece = (256 << 20) // flat.element_size()
+    s = torch.cuda.Stream(dev)
+    best = 0.0
+    with torch.cuda.stream(s):
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            for off in range(0, flat.numel(), piece):
+                dst[off:off + piece].copy_(flat[off:off + piece], non_blocking=True)
+            e1.record(s)
+            e1.synchronize()
+            best = max(best, flat.numel() * flat.element_size() / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del dst
+    return best
+
+
 def load_traffic(workload: str):
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
@@ -323,10 +439,15 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     cells = n * w
     esize = 4 if field == 0 else 8
     pcs = Z.CudaTwoAdicPcs(field, P2_SEED, lb, wl["p2w"])
-    trace = make_trace(torch, wl, dev)
+    # the seeded trace (the one tests/golden/fullsize.json answers for), in pinned host memory
+    # first touched by the GPU's local CPUs
+    local = GpuLocalMemory(torch, local_rank)
+    with local:
+        pinned = torch.empty((n, w), dtype=torch.int32 if field == 0 else torch.int64).pin_memory()
+        synthetic_trace(field, n, w, TRACE_SEED, out=pinned.numpy().view(np.uint32 if field == 0 else np.uint64))
+    trace = pinned.to(dev)
     torch.cuda.synchronize()
-    pinned = torch.empty_like(trace, device="cpu").pin_memory()
-    pinned.copy_(trace)
+    h2d_gbs = measure_h2d(torch, pinned, dev)
     root = np.zeros(pcs.mmcs.digest_elems, dtype=np.uint32 if field == 0 else np.uint64)
     stream = torch.cuda.current_stream(dev)
     with_fri = field == 0
@@ -335,7 +456,7 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         if with_fri:
             _, _, pf = pcs.commit_fri_dev(trace, ALPHA, FRI["log_final"], FRI["num_queries"],
                                           FRI["challenge_seed"], FRI["query_seed"], want_tree=False, root=root)
-            return pf.roots.copy()
+            return pf
         pcs.commit_dev(trace, want_tree=False, root=root)
         return None
 
@@ -364,7 +485,7 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        fri_roots = step_dev()
+        last_pf = step_dev()
     ev1.record(stream)
     ev1.synchronize()
     barrier()
@@ -372,8 +493,9 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     clocks = sampler.stop() if sampler else None
     t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     assert (root == root_ref).all(), "root changed between steps"
-    assert not with_fri or (fri_roots == fri_ref).all(), "FRI commitments changed between steps"
+    assert not with_fri or (last_pf.roots == fri_ref.roots).all(), "FRI commitments changed between steps"
     gpu_launches = sum(v[0] for v in kstats.values())
+    parity = golden_check(args.workload, wl, root, last_pf)
 
     # ---- end-to-end timed region: pinned host trace -> root and FRI answers on the host,
     # through the serving engine (the copy of one job overlaps the kernels of another)
@@ -398,6 +520,7 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     fri_d2h = 4 * (8 * rounds + 4 * rounds + 4 * (1 << FRI["log_final"]) + FRI["num_queries"] * (
         2 + 8 * rounds + 8 * sum(wl["log_h"] + lb - r - 1 for r in range(rounds))))
     e2e = cells * args.steps * world / t_e2e
+    ceiling_ms = max(1e3 * t_dev / args.steps, cells * esize / (h2d_gbs * 1e9) * 1e3)
     # roofline of the dominant kernel (leaf sponge hashing; integer-multiply bound)
     N_rows = n << lb
     leaf_perms, comp_perms = perms_of_commit(wl["log_h"] + lb, w)
@@ -453,8 +576,10 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         for _ in range(2):
             dt, c = cpu_commit_sample(wl, log_rows, threads)
             dts.append(dt)
+        job = f"LDE x2^{lb} + MMCS" + (" + alpha-reduction + FRI commit phase and queries" if with_fri else "")
         cpu = {"value": c / min(dts), "unit": "cells/s", "cores": threads, "kind": "port",
-               "sample": f"2^{log_rows} x {w} trace (LDE x2^{lb} + MMCS), best of 2, oracle/ C restatement"}
+               "sample": f"2^{log_rows} x {w} trace ({job}), best of 2, oracle/ C restatement with scalar "
+                         "remainder arithmetic (not p3's packed-SIMD kernels)"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
@@ -469,7 +594,12 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         "e2e": {"value": e2e, "unit": "cells/s", "h2d_bytes_per_step": cells * esize,
                 "d2h_bytes_per_step": int(root.nbytes) + (fri_d2h if with_fri else 0),
                 "ms_per_step": 1e3 * t_e2e / args.steps, "path": f"zkb_engine_submit/wait, {E2E_SLOTS} slots",
-                "latency_ms_p50": e2e_lat[len(e2e_lat) // 2], "latency_ms_max": e2e_lat[-1]},
+                "latency_ms_p50": e2e_lat[len(e2e_lat) // 2], "latency_ms_max": e2e_lat[-1],
+                "h2d_gbs_measured": h2d_gbs, "pinned_memory": local.describe(),
+                "ceiling_ms": ceiling_ms, "frac_of_ceiling": ceiling_ms / (1e3 * t_e2e / args.steps),
+                "ceiling": "max(device ms/step, trace bytes / measured pinned H2D bandwidth): the copy of "
+                           "one job hidden under another's kernels"},
+        "parity": parity,
         "roofline": roofline,
         "roofline_ntt": ntt_roof,
         "step": "LDE + Poseidon2 MMCS" + (" + alpha-reduction + FRI (2^%d -> 2^%d, %d queries)" % (
