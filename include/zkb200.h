@@ -86,6 +86,10 @@ ZKB_API int zkb_get_thresholds(zkb_thresholds *thresholds_out);
  * next `count` device allocations fail as out of memory; kind 2: the next `count` stream
  * waits report an expired deadline (after the work has finished). */
 ZKB_API int zkb_debug_inject_fault(int kind, int count);
+/* Number of device allocations (stream-ordered pool or cudaMalloc) the library has
+ * made in this process.  Tests read it around a call to check that the call allocated
+ * nothing.  No counterpart in the reference. */
+ZKB_API uint64_t zkb_debug_device_allocations(void);
 
 /* Kernel timing.  zkb_profile_start() enables per-launch CUDA events (recorded on
  * the stream each kernel is launched on) and clears earlier records;

@@ -107,3 +107,40 @@ def test_lde_goldilocks_full_size_columns(oracle):
     assert not coef[n:].any()
     # the low coefficients are the trace's, scaled by shift^m
     assert coef[:n].any()
+
+
+def test_ntt_accelerator_name_and_availability():
+    """zkf-metal/src/ntt/mod.rs:114-120 (metal_ntt_accelerator_available)."""
+    acc = Z.CudaNttAccelerator.new()
+    assert acc is not None and acc.name() == "cuda-b200-ntt" and acc.is_available()
+    assert acc.max_log_size() == 26
+
+
+def test_ntt_accelerator_forward_inverse_roundtrip(oracle):
+    """zkf-metal/src/ntt/mod.rs:122-145: values 1..2^13 forward then inverse; the forward
+    result is also compared with the oracle's width-1 Goldilocks DFT (the call the
+    NttAccelerator shim makes: zkb_dft_batch(GOLDILOCKS, ..., width 1, inverse))."""
+    acc = Z.CudaNttAccelerator()
+    n = 1 << 13
+    values = [i + 1 for i in range(n)]
+    original = list(values)
+    acc.forward_ntt(values)
+    assert values != original
+    want = oracle.dft_batch(Z.GOLDILOCKS, np.arange(1, n + 1, dtype=np.uint64).reshape(-1, 1))
+    assert values == [int(x) for x in want[:, 0]]
+    acc.inverse_ntt(values)
+    assert values == original
+
+
+def test_ntt_accelerator_reduces_inputs_and_rejects_bad_sizes(oracle):
+    """Inputs above p are taken mod p after truncation to 64 bits (Goldilocks::from_u64 of
+    the low 8 bytes); sizes that are not powers of two are errors, as in the reference."""
+    acc = Z.CudaNttAccelerator()
+    big = [GL_P + 5, (1 << 64) + 3, GL_P - 1, 0]
+    acc.forward_ntt(big)
+    want = oracle.dft_batch(Z.GOLDILOCKS, np.array([5, 3, GL_P - 1, 0], np.uint64).reshape(-1, 1))
+    assert big == [int(x) for x in want[:, 0]]
+    with pytest.raises(Z.ZkbError):
+        acc.forward_ntt([1, 2, 3])
+    with pytest.raises(Z.ZkbError):
+        acc.inverse_ntt([])

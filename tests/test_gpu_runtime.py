@@ -47,6 +47,24 @@ def test_lde_merkle_fri_query_graph(oracle):
     assert all(rt.node_ms(n) >= 0 for n in (lde, mk, fold, mk2, q))
 
 
+def test_query_index_past_the_tree_is_an_error():
+    """Query indices come from a device buffer; one past the tree is reported (query
+    number, index, tree height) instead of opening some other row."""
+    rt = Z.ProverRuntime()
+    R = Z.ProverRuntime
+    m = rand_field(Z.BABYBEAR, (1 << 6, 8), 64)
+    s_m = rt.buffer(m.nbytes)
+    rt.write(s_m, m)
+    mk = rt.add(R.MERKLE, log_n=6, width=8, in_slot=s_m)
+    idx = np.array([3, 63, 64, 7], np.uint64)
+    s_idx, s_open = rt.buffer(idx.nbytes), rt.buffer(len(idx) * (8 + 6 * 8) * 4)
+    rt.write(s_idx, idx)
+    rt.add(R.FRI_QUERY_OPEN, deps=[mk], count=len(idx), in_slot=s_idx, out_slot=s_open, tree_node=mk)
+    with pytest.raises(Z.ZkbError) as e:
+        rt.execute()
+    assert e.value.code == N.ERR_INVALID and "query 2 opens row 64 of a 64-row tree" in str(e.value)
+
+
 def test_ntt_and_poseidon_nodes(oracle):
     rt = Z.ProverRuntime()
     R = Z.ProverRuntime

@@ -13,6 +13,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import ziros_b200 as Z
 from conftest import rand_field
 from ziros_b200 import _native as N
 
@@ -41,6 +42,37 @@ def test_noalloc_matches_allocating_entry_point_twice(field):
         got = _run("zkb_dft_batch_noalloc_dev", field, m, inverse)
         want = _run("zkb_dft_batch_dev", field, m, inverse)
         assert (got == want).all()
+
+
+@pytest.mark.parametrize("field", [0, 1])
+def test_noalloc_makes_no_device_allocation(field):
+    """The library counts every device allocation it makes; a shape no other call has
+    used (so no cached table exists for it) must leave the count unchanged."""
+    m = rand_field(field, (1 << 11, 5), 8)
+    before = N.device_allocations()
+    got = _run("zkb_dft_batch_noalloc_dev", field, m, True)
+    assert N.device_allocations() == before
+    assert (got == _run("zkb_dft_batch_dev", field, m, True)).all()
+    assert N.device_allocations() > before  # the allocating entry point is counted
+
+
+def test_noalloc_declines_while_circuit_open():
+    """Like every entry point, it does no GPU work while the circuit is open."""
+    import torch
+
+    t = torch.zeros((1 << 6, 2), dtype=torch.int32, device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    lib = N.load()
+    N.inject_fault(2, 1)  # the next stream wait reports an expired deadline: the circuit opens
+    try:
+        with pytest.raises(N.ZkbError):
+            Z.CudaDft(0).dft_batch(rand_field(0, (1 << 6, 2), 1))
+        assert lib.zkb_dft_batch_noalloc_dev(0, C.c_void_p(t.data_ptr()), 6, 2, 0, stream) == N.DECLINED
+        assert "circuit open" in N.last_error()
+    finally:
+        N.inject_fault(2, 0)
+        N.circuit_reset()
+    N.check(lib.zkb_dft_batch_noalloc_dev(0, C.c_void_p(t.data_ptr()), 6, 2, 0, stream))
 
 
 def test_noalloc_rejects_sizes_beyond_scratch():

@@ -17,6 +17,7 @@ from .accel import (  # noqa: F401
     FriProof,
     combine_columns_dev,
     CudaMerkleTreeMmcs,
+    CudaNttAccelerator,
     CudaPolyOps,
     CudaPoseidon2,
     CudaTwoAdicPcs,

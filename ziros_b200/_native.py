@@ -179,6 +179,7 @@ SIGNATURES = {
     "zkb_circuit_open": (_I, [C.c_char_p, _SZ]),
     "zkb_circuit_reset": (None, []),
     "zkb_debug_inject_fault": (_I, [_I, _I]),
+    "zkb_debug_device_allocations": (_U64, []),
     "zkb_engine_cancel": (_I, [_P, _U64]),
     "zkb_mmcs_verify_batch": (_I, [_P, _P, _P, _P, _SZ, _U64, _P, _P, _SZ]),
     "zkb_challenger_create": (_I, [_P, _P]),
@@ -249,6 +250,11 @@ def circuit_reset() -> None:
 def inject_fault(kind: int, count: int = 1) -> None:
     """Host-side fault injection for tests (1: allocations fail, 2: waits time out)."""
     check(load().zkb_debug_inject_fault(kind, count))
+
+
+def device_allocations() -> int:
+    """Device allocations the library has made in this process (pool or cudaMalloc)."""
+    return int(load().zkb_debug_device_allocations())
 
 
 def last_error() -> str:

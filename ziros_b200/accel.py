@@ -171,6 +171,48 @@ class CudaDft:
                                                  c_fused, op, stream))
 
 
+class CudaNttAccelerator:
+    """NttAccelerator (zkf-core/src/acceleration.rs:62-81) as MetalNttAccelerator
+    implements it (zkf-metal/src/ntt/mod.rs:13-109): a Goldilocks transform of one
+    column, natural order in place.  Each value's low 64 bits are reduced into the
+    field (Goldilocks::from_u64 of the first 8 little-endian bytes), the transform runs
+    through zkb_dft_batch(GOLDILOCKS, width 1) and the canonical results are written
+    back.  forward_ntt is the DFT, inverse_ntt the inverse DFT with the 1/n scale."""
+
+    def __init__(self):
+        N.load()
+
+    @staticmethod
+    def new() -> Optional["CudaNttAccelerator"]:
+        N.load()
+        return CudaNttAccelerator() if _have_device() else None
+
+    def name(self) -> str:
+        return "cuda-b200-ntt"
+
+    def is_available(self) -> bool:
+        return _have_device()
+
+    def max_log_size(self) -> int:
+        return 26
+
+    def _run(self, values: list, inverse: int) -> None:
+        n = len(values)
+        if n == 0 or n & (n - 1):
+            raise N.ZkbError(N.ERR_INVALID, "NTT size must be a power of 2")
+        if n.bit_length() - 1 > self.max_log_size():
+            raise N.ZkbError(N.ERR_INVALID, f"NTT of 2^{n.bit_length() - 1} exceeds max_log_size 2^26")
+        v = np.array([(int(x) & 0xFFFFFFFFFFFFFFFF) % GL_P for x in values], dtype=np.uint64)
+        N.check(N.load().zkb_dft_batch(GOLDILOCKS, _ptr(v), n.bit_length() - 1, 1, inverse))
+        values[:] = [int(x) for x in v]
+
+    def forward_ntt(self, values: list) -> None:
+        self._run(values, 0)
+
+    def inverse_ntt(self, values: list) -> None:
+        self._run(values, 1)
+
+
 # -------------------------------------------------------------------------- MMCS
 class Tree:
     """Prover data of a commitment (p3 MerkleTree): digest layers stay on the device."""

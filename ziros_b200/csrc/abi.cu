@@ -165,6 +165,8 @@ int zkb_debug_inject_fault(int kind, int count) {
   return rc;
 }
 
+uint64_t zkb_debug_device_allocations(void) { return device_alloc_count(); }
+
 int zkb_set_device(int device) {
   clear_error();
   ZKB_CHECK_CUDA(cudaSetDevice(device));

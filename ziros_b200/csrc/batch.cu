@@ -235,6 +235,7 @@ struct zkb_batch {
     d_coef.clear();
     coef_bytes = 0;
     void *scratch = nullptr;
+    note_device_alloc();
     ZKB_CHECK_CUDA(cudaMalloc(&scratch, total));
     d_coef.push_back(scratch);
     for (uint32_t b = 1; b < nb; b++) d_coef.push_back((char *)d_coef[b - 1] + need[b - 1]);
@@ -505,6 +506,7 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   ZKB_REQUIRE(b->arena_bytes + (1ull << 30) <= free_b,
               "batch needs %llu bytes of device memory, %llu free", (unsigned long long)b->arena_bytes,
               (unsigned long long)free_b);
+  note_device_alloc();
   ZKB_CHECK_CUDA(cudaMalloc(&b->arena, b->arena_bytes));
   char *base = (char *)b->arena;
   b->d_in.resize(n);

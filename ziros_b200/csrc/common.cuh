@@ -74,6 +74,10 @@ inline cudaStream_t resolve_stream(void *s) { return (cudaStream_t)s; }
 
 // Stream-ordered scratch allocation from the device's memory pool.
 int dev_alloc(void **p, size_t bytes, cudaStream_t s);
+// Every device allocation the library makes (pool or cudaMalloc) is counted here;
+// zkb_debug_device_allocations() reads the count.
+void note_device_alloc();
+uint64_t device_alloc_count();
 // Host wait on a stream with the watchdog deadline (ZKB_WATCHDOG_MS, default 120 s, 0 =
 // none); a device error or an expired deadline opens the circuit.
 int wait_stream(cudaStream_t s);

@@ -355,7 +355,15 @@ void set_thresholds(const zkb_thresholds &t) {
   g_thr = t;
 }
 
+namespace {
+std::atomic<uint64_t> g_device_allocs{0};
+}
+
+void note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
+uint64_t device_alloc_count() { return g_device_allocs.load(std::memory_order_relaxed); }
+
 int dev_alloc(void **p, size_t bytes, cudaStream_t s) {
+  note_device_alloc();
   if (take_injected(g_inject_oom)) {
     *p = nullptr;
     set_error("device allocation of %zu bytes failed: out of memory (injected)", bytes);

@@ -28,25 +28,57 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 namespace {
 std::mutex g_scratch_mu;
-void *g_scratch_dev[64] = {nullptr};
+struct ScratchSlot {
+  void *ctx = nullptr;  // CUcontext the address belongs to
+  void *ptr = nullptr;
+};
+ScratchSlot g_scratch_dev[64];
 
-// The symbol's name is a host-side stand-in, not a device address.  The address is
-// looked up once per device with that device current (first call on the device).
+// cuCtxGetCurrent, fetched from the driver at run time (the library does not link
+// libcuda, so it still loads on a machine without a driver).
+using CtxGetCurrentFn = int (*)(void **);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (CtxGetCurrentFn) nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+void *current_ctx() {
+  void *c = nullptr;
+  CtxGetCurrentFn fn = ctx_get_current();
+  if (!fn || fn(&c) != 0) return nullptr;
+  return c;
+}
+
+// The symbol's name is a host-side stand-in, not a device address.  Set-up, once per
+// device with that device current (the first call on the device): cudaGetSymbolAddress
+// gives the array's address in the device's context.  The address is kept with the
+// context it belongs to; if the context was torn down and re-created (cudaDeviceReset),
+// the module was reloaded elsewhere and the lookup runs again.
 int scratch_address(void **out) {
   int dev = 0;
   ZKB_CHECK_CUDA(cudaGetDevice(&dev));
   ZKB_REQUIRE(dev >= 0 && dev < 64, "device ordinal %d out of range", dev);
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_dev[dev]) {
+  ScratchSlot &slot = g_scratch_dev[dev];
+  void *ctx = current_ctx();
+  if (!slot.ptr || ctx == nullptr || ctx != slot.ctx) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) {
       set_error("cudaGetSymbolAddress of the allocation-free scratch failed: %s", cudaGetErrorString(e));
       return ZKB_ERR_CUDA;
     }
-    g_scratch_dev[dev] = p;
+    slot.ptr = p;
+    slot.ctx = current_ctx();  // the lookup made the device's primary context current
   }
-  *out = g_scratch_dev[dev];
+  *out = slot.ptr;
   return ZKB_OK;
 }
 
@@ -77,6 +109,7 @@ extern "C" int zkb_dft_batch_noalloc_dev(int field, void *d_rowmajor, uint32_t l
                                          int inverse, void *stream) {
   using namespace zkb;
   clear_error();
+  ZKB_TRY(library_gate());  // kill switch and open circuit decline, as in every entry point
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
     set_error("no CUDA device available");

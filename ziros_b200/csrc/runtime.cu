@@ -19,15 +19,22 @@
 namespace zkb {
 namespace {
 
-// Rows of a committed matrix and their sibling paths, one thread per query.
+// Rows of a committed matrix and their sibling paths, one thread per query.  The indices
+// live in a device buffer the host has not seen: a query whose index is past the tree
+// opens nothing and records itself in *bad (the smallest such query number), which the
+// host reads and reports as an error.
 template <class T, int OUT>
 __global__ void open_rows_kernel(const T *__restrict__ leaves, uint64_t rows, uint32_t width,
                                  const T *__restrict__ layers, const uint64_t *__restrict__ layer_off, int depth,
-                                 const uint64_t *__restrict__ idx, int n, T *__restrict__ out) {
+                                 const uint64_t *__restrict__ idx, int n, T *__restrict__ out,
+                                 unsigned long long *bad) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
-  uint64_t i = idx[q];
-  if (i >= rows) i = rows - 1;  // the indices live in a device buffer: an index past the tree opens its last row
+  const uint64_t i = idx[q];
+  if (i >= rows) {
+    atomicMin(bad, (unsigned long long)q);
+    return;
+  }
   T *o = out + (uint64_t)q * (width + (uint64_t)depth * OUT);
   for (uint32_t c = 0; c < width; c++) o[c] = leaves[i * width + c];
   for (int l = 0; l < depth; l++) {
@@ -150,15 +157,31 @@ struct zkb_rt {
         ZKB_TRY(slot(n.in_slot, n.count * 8, &in));
         ZKB_TRY(slot(n.out_slot, n.count * (tw + (uint64_t)depth * out_d) * es, &out));
         if (n.count == 0) return ZKB_OK;
+        ZKB_REQUIRE(n.count <= 0x7fffffffull, "query node %d: %llu queries", id, (unsigned long long)n.count);
+        // scratch: the layer offsets, then the bad-query word (all ones: none)
         ScratchBuf d_off;
-        ZKB_TRY(d_off.alloc((depth + 1) * 8, s));
-        ZKB_CHECK_CUDA(cudaMemcpyAsync(d_off.p, dt.layer_off.data(), (depth + 1) * 8, cudaMemcpyHostToDevice, s));
+        ZKB_TRY(d_off.alloc((depth + 2) * 8, s));
+        std::vector<uint64_t> hbuf(dt.layer_off.begin(), dt.layer_off.begin() + depth + 1);
+        hbuf.push_back(~0ull);
+        ZKB_CHECK_CUDA(cudaMemcpyAsync(d_off.p, hbuf.data(), (depth + 2) * 8, cudaMemcpyHostToDevice, s));
+        unsigned long long *d_bad = reinterpret_cast<unsigned long long *>(d_off.as<uint64_t>() + depth + 1);
         const unsigned grid = (unsigned)((n.count + 127) / 128);
         if (out_d == 8)
-          ZKB_LAUNCH("rt_query_open", s, open_rows_kernel<T, 8><<<grid, 128, 0, s>>>((const T *)dt.mats[0].data, trows, (uint32_t)tw, (const T *)dt.d_layers, d_off.as<uint64_t>(), depth, (const uint64_t *)in, (int)n.count, (T *)out));
+          ZKB_LAUNCH("rt_query_open", s, open_rows_kernel<T, 8><<<grid, 128, 0, s>>>((const T *)dt.mats[0].data, trows, (uint32_t)tw, (const T *)dt.d_layers, d_off.as<uint64_t>(), depth, (const uint64_t *)in, (int)n.count, (T *)out, d_bad));
         else
-          ZKB_LAUNCH("rt_query_open", s, open_rows_kernel<T, 4><<<grid, 128, 0, s>>>((const T *)dt.mats[0].data, trows, (uint32_t)tw, (const T *)dt.d_layers, d_off.as<uint64_t>(), depth, (const uint64_t *)in, (int)n.count, (T *)out));
-        return wait_stream(s);  // the layer offsets are read before the scratch is released
+          ZKB_LAUNCH("rt_query_open", s, open_rows_kernel<T, 4><<<grid, 128, 0, s>>>((const T *)dt.mats[0].data, trows, (uint32_t)tw, (const T *)dt.d_layers, d_off.as<uint64_t>(), depth, (const uint64_t *)in, (int)n.count, (T *)out, d_bad));
+        unsigned long long bad = 0;
+        ZKB_CHECK_CUDA(cudaMemcpyAsync(&bad, d_bad, 8, cudaMemcpyDeviceToHost, s));
+        // the layer offsets and the bad-query word are read before the scratch is released
+        ZKB_TRY(wait_stream(s));
+        if (bad != ~0ull) {
+          uint64_t bad_idx = 0;
+          ZKB_CHECK_CUDA(cudaMemcpy(&bad_idx, (const uint64_t *)in + bad, 8, cudaMemcpyDeviceToHost));
+          set_error("query node %d: query %llu opens row %llu of a %llu-row tree", id, bad,
+                    (unsigned long long)bad_idx, (unsigned long long)trows);
+          return ZKB_ERR_INVALID;
+        }
+        return ZKB_OK;
       }
       default:
         set_error("unknown node kind %d", n.kind);
@@ -190,6 +213,7 @@ int zkb_rt_buffer(zkb_rt *rt, uint64_t bytes, int *slot_out) {
   ZKB_REQUIRE(rt && slot_out && bytes > 0, "invalid arguments");
   ZKB_CHECK_CUDA(cudaSetDevice(rt->device));
   void *p = nullptr;
+  note_device_alloc();
   ZKB_CHECK_CUDA(cudaMalloc(&p, bytes));
   rt->bufs.emplace_back(p, bytes);
   *slot_out = (int)rt->bufs.size() - 1;
