@@ -110,6 +110,7 @@ static int table_build_allowed(cudaStream_t s) {
 // Table memory lives as long as the process and is allocated outside the stream-ordered
 // pool, so permanent blocks do not fragment the pool that jobs allocate from and free to.
 static int table_alloc(void **p, size_t bytes) {
+  note_device_alloc();
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -397,10 +398,13 @@ __global__ void __launch_bounds__(C << LR2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
   // Twiddles shared by the C columns of the CTA, staged once:
-  //   tw_in[i*R1 + t]  = w_{2^K}^{i * rev(t)}   (phase-A twist of output t of thread i)
+  //   tw_in[i*TP + t]  = w_{2^K}^{i * rev(t)}   (phase-A twist of output t of thread i; rows
+  //                      padded to TP = R1 + 1 entries so the distinct i of a warp hit
+  //                      distinct banks)
   //   tw_out[f]        = w_{2^hi}^{i_low * f}  (pass twist), or the 1/n scale on the last pass
+  constexpr int TP = R1 + 1;
   TwS<F> *tw_in = reinterpret_cast<TwS<F> *>(sm + S * R1);
-  TwS<F> *tw_out = tw_in + (1 << K);
+  TwS<F> *tw_out = tw_in + R2 * TP;
 
   const uint32_t cta = blockIdx.x;
   const uint32_t chunk = cta % g.chunks_per_row;
@@ -416,7 +420,7 @@ __global__ void __launch_bounds__(C << LR2)
 
   for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) {
     const uint32_t ii = e / R1, tt = e % R1;
-    tw_in[e] = tw_stage<F>(tw[(ii * (__brev(tt) >> (32 - LR1))) << (g.L - K)]);
+    tw_in[ii * TP + tt] = tw_stage<F>(tw[(ii * (__brev(tt) >> (32 - LR1))) << (g.L - K)]);
     if (g.twist)
       tw_out[e] = tw_stage<F>(tw[(i_low * e) << (g.L - hi)]);  // i_low * e < 2^hi <= 2^L
     else if (post_scale)
@@ -438,7 +442,7 @@ __global__ void __launch_bounds__(C << LR2)
     }
     dif_reg<F, LR1>(x, st);
     __syncthreads();  // tw_in staged
-    const TwS<F> *twi = tw_in + i * R1;
+    const TwS<F> *twi = tw_in + i * TP;
     sfor<R1>([&](auto tc) {
       constexpr int t = decltype(tc)::value;
       T v = x[t];
@@ -521,7 +525,7 @@ static int launch_pass_c(const typename F::T *src, typename F::T *out, const Pas
   using T = typename F::T;
   constexpr unsigned threads = C << LR2;
   const size_t smem = (size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) * sizeof(T) +
-                      (size_t)(2u << (LR1 + LR2)) * sizeof(TwS<F>);
+                      (size_t)(((1u << LR2) * ((1u << LR1) + 1)) + (1u << (LR1 + LR2))) * sizeof(TwS<F>);
   ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<F, LR1, LR2, C>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   ZKB_LAUNCH("ntt_pass", s, ntt_pass_kernel<F, LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(src, out, g, tw, scale, st));
@@ -659,9 +663,10 @@ __global__ void __launch_bounds__(C << LR2)
   constexpr int S = PassSmem<LR2, C>::STRIDE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
+  constexpr int TP = R1 + 1;  // padded [i][t] rows: the distinct i of a warp hit distinct banks
   TwS<F> *itw_in = reinterpret_cast<TwS<F> *>(sm + S * R1);  // [i][t] inverse inner twist
-  TwS<F> *ftw_in = itw_in + (1 << K);                        // [i][t] forward inner twist
-  TwS<F> *ftw_out = ftw_in + (1 << K);                       // w_{2^L}^{m_lo * f}
+  TwS<F> *ftw_in = itw_in + R2 * TP;                         // [i][t] forward inner twist
+  TwS<F> *ftw_out = ftw_in + R2 * TP;                        // w_{2^L}^{m_lo * f}
   TwS<F> *cf = ftw_out + (1 << K);                           // coset factors of the current coset
 
   const uint32_t cta = blockIdx.x;
@@ -675,8 +680,8 @@ __global__ void __launch_bounds__(C << LR2)
   for (uint32_t e = threadIdx.x; e < (1u << K); e += blockDim.x) {
     const uint32_t ii = e / R1, tt = e % R1;
     const uint32_t ex = (ii * (__brev(tt) >> (32 - LR1))) << lm;
-    itw_in[e] = tw_stage<F>(itw[ex]);
-    ftw_in[e] = tw_stage<F>(ftw[ex]);
+    itw_in[ii * TP + tt] = tw_stage<F>(itw[ex]);
+    ftw_in[ii * TP + tt] = tw_stage<F>(ftw[ex]);
     ftw_out[e] = tw_stage<F>(ftw_t[((size_t)m_lo << K) + e]);  // w^(m_lo * e), contiguous per m_lo
   }
 
@@ -695,7 +700,7 @@ __global__ void __launch_bounds__(C << LR2)
     }
     dif_reg<F, LR1>(x, ist);
     __syncthreads();
-    const TwS<F> *twi = itw_in + i * R1;
+    const TwS<F> *twi = itw_in + i * TP;
     sfor<R1>([&](auto tc) {
       constexpr int t = decltype(tc)::value;
       T v = x[t];
@@ -729,7 +734,7 @@ __global__ void __launch_bounds__(C << LR2)
 #pragma unroll
       for (int j = 0; j < R1; j++) x[j] = tw_mul<F>(coef[j], cf[j * R2 + i]);
       dif_reg<F, LR1>(x, fst);
-      const TwS<F> *twi = ftw_in + i * R1;
+      const TwS<F> *twi = ftw_in + i * TP;
       sfor<R1>([&](auto tc) {
         constexpr int t = decltype(tc)::value;
         T v = x[t];
@@ -768,7 +773,7 @@ static int launch_fused_c(const typename F::T *in, typename F::T *out, const Fus
   using T = typename F::T;
   constexpr unsigned threads = C << LR2;
   const size_t smem = (size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) * sizeof(T) +
-                      (size_t)(4u << (LR1 + LR2)) * sizeof(TwS<F>);
+                      (size_t)(2u * ((1u << LR2) * ((1u << LR1) + 1)) + (2u << (LR1 + LR2))) * sizeof(TwS<F>);
   ZKB_CHECK_CUDA(cudaFuncSetAttribute(lde_fused_kernel<F, LR1, LR2, C>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   const uint64_t ctas = (uint64_t)g.chunks_per_row * g.blocks;
