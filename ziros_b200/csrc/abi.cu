@@ -390,7 +390,8 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
                     uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out,
                     cudaStream_t s, const uint32_t *alpha = nullptr, const zkb_fri_params *fri = nullptr,
                     FriProof *fri_out = nullptr, UploadGate *upload_mu = nullptr,
-                    std::unique_lock<std::mutex> *compute_lock = nullptr) {
+                    std::unique_lock<std::mutex> *compute_lock = nullptr, JobStages *stages = nullptr,
+                    cudaStream_t fri_s = nullptr) {
   ZKB_REQUIRE(log_h + log_blowup < 40, "size too large");
   const size_t es = field_elem_bytes(spec.field);
   const uint64_t n = 1ull << log_h, N = n << log_blowup;
@@ -425,9 +426,11 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
     }
     d_trace = staged.p;
   }
+  if (stages) stages->uploaded = std::chrono::steady_clock::now();
   // an engine job waits here, its trace on the device, until the jobs of its size class
   // ahead of it have finished computing
   if (compute_lock) compute_lock->lock();
+  if (stages) stages->lock_taken = std::chrono::steady_clock::now();
   void *lde = nullptr;
   ZKB_TRY(dev_alloc(&lde, N * width * es, s));
   tree->t.owned.push_back(lde);
@@ -471,8 +474,24 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
     ZKB_TRY(wait_stream(s));
     compute_lock->unlock();
   }
+  if (stages) stages->tree_built = std::chrono::steady_clock::now();
   if (fri) {
-    // alpha-reduction of the committed columns (unless fused above), then the FRI commit phase
+    // alpha-reduction of the committed columns (unless fused above), then the FRI commit phase,
+    // on fri_s when given: ordered after the tree by an event, and s waits for it before
+    // anything of the job is read back or freed
+    struct EventHolder {
+      cudaEvent_t e = nullptr;
+      ~EventHolder() {
+        if (e) cudaEventDestroy(e);
+      }
+    } ev;
+    cudaStream_t fs = s;
+    if (fri_s && fri_s != s) {
+      ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
+      ZKB_CHECK_CUDA(cudaEventRecord(ev.e, s));
+      ZKB_CHECK_CUDA(cudaStreamWaitEvent(fri_s, ev.e, 0));
+      fs = fri_s;
+    }
     const int log_n = (int)(log_h + log_blowup);
     DuplexChallenger ch;
     uint32_t a[4];
@@ -488,10 +507,14 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
       for (int k = 0; k < 4; k++) a[k] = alpha[k];
     }
     for (int k = 0; k < 4; k++) fri_out->alpha[k] = a[k];
-    if (!fused_reduction) ZKB_TRY(combine_columns_ext4_dev((const uint32_t *)lde, N, width, a, (uint32_t *)cw, s));
+    if (!fused_reduction) ZKB_TRY(combine_columns_ext4_dev((const uint32_t *)lde, N, width, a, (uint32_t *)cw, fs));
     ZKB_TRY(fri_commit_ext4_dev(spec, (const uint32_t *)cw, log_n, (int)fri->log_final,
-                                fri->challenge_seed, (int)fri->num_queries, fri->query_seed, fri_out, s,
+                                fri->challenge_seed, (int)fri->num_queries, fri->query_seed, fri_out, fs,
                                 fri->transcript ? &ch : nullptr));
+    if (fs != s) {
+      ZKB_CHECK_CUDA(cudaEventRecord(ev.e, fs));
+      ZKB_CHECK_CUDA(cudaStreamWaitEvent(s, ev.e, 0));
+    }
   }
   return tree_from(tree_out, tree, root_out, s);
 }
@@ -503,11 +526,12 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
 // before returning.
 int zkb::pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                      uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
-                     FriProof *fri_out, cudaStream_t s, UploadGate *upload_mu, std::mutex *compute_mu) {
+                     FriProof *fri_out, cudaStream_t s, UploadGate *upload_mu, std::mutex *compute_mu,
+                     JobStages *stages, cudaStream_t fri_stream) {
   std::unique_lock<std::mutex> cl;
   if (compute_mu) cl = std::unique_lock<std::mutex>(*compute_mu, std::defer_lock);
   int rc = pcs_commit_impl(spec, nullptr, h_trace, log_h, width, log_blowup, root_out, nullptr, s,
-                           alpha, fri, fri_out, upload_mu, compute_mu ? &cl : nullptr);
+                           alpha, fri, fri_out, upload_mu, compute_mu ? &cl : nullptr, stages, fri_stream);
   if (fri_out) fri_out->release_device();
   if (rc == ZKB_OK) ZKB_TRY(wait_stream(s));
   return rc;  // the compute lock (if taken) is released here, after the job's work

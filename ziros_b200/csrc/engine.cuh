@@ -1,5 +1,6 @@
 // engine.cuh — internal host-side interfaces between the CUDA modules.
 #pragma once
+#include <chrono>
 #include <array>
 #include <condition_variable>
 #include <memory>
@@ -166,11 +167,18 @@ class UploadGate {
 // upload_mu (may be NULL) serialises the host-to-device copies of concurrent jobs, taken
 // per piece of the trace; compute_mu (may be NULL) is held from the end of the upload until
 // the job's tree is built, so jobs sharing it run their large kernels one at a time while
-// others upload (and their FRI phases overlap the next job's LDE).
+// others upload (and their FRI phases overlap the next job's LDE).  fri_stream (may be NULL:
+// s) runs the FRI phase; the engine gives it a higher priority than the next job's LDE and
+// tree, whose long kernels would otherwise hold back its chain of small ones.
+// Host times (steady clock) at which an engine job's stages ended, for the job log.
+struct JobStages {
+  std::chrono::steady_clock::time_point uploaded, lock_taken, tree_built;
+};
 int pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                 uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
                 FriProof *fri_out, cudaStream_t s, UploadGate *upload_mu = nullptr,
-                std::mutex *compute_mu = nullptr);
+                std::mutex *compute_mu = nullptr, JobStages *stages = nullptr,
+                cudaStream_t fri_stream = nullptr);
 int combine_columns_ext4_dev(const uint32_t *d_lde, uint64_t rows, uint32_t width,
                              const uint32_t alpha[4], uint32_t *d_out, cudaStream_t s);
 // With `ch` set, every round's root is observed before its beta is sampled, the final

@@ -57,6 +57,7 @@ struct Job {
   HasherSpec spec;
   uint64_t mem_estimate = 0;
   Clock::time_point t_submit, t_start, t_done;
+  JobStages stages;
   uint32_t bypassed = 0;  // times a younger job was admitted while this one waited
   int status = 1;  // 1 queued / running, 0 done, <0 error
   std::string error;
@@ -66,6 +67,11 @@ struct Job {
 
 // ZKB_JOB_LOG=<path>: one JSON line per finished job (shape, status, queue/run/latency ms,
 // cells), appended, for per-job metrics next to the p50/p99 the caller computes.
+Clock::time_point log_epoch() {
+  static const Clock::time_point t0 = Clock::now();
+  return t0;
+}
+
 void log_job(const Job &j, int rc, Clock::time_point done) {
   static const char *path = getenv("ZKB_JOB_LOG");
   if (!path || !*path) return;
@@ -76,10 +82,16 @@ void log_job(const Job &j, int rc, Clock::time_point done) {
   if (!f) return;
   fprintf(f,
           "{\"job\": %llu, \"field\": %d, \"log_h\": %u, \"width\": %u, \"log_blowup\": %u, \"fri\": %d, "
-          "\"status\": %d, \"cells\": %llu, \"queue_ms\": %.3f, \"run_ms\": %.3f, \"latency_ms\": %.3f}\n",
+          "\"status\": %d, \"cells\": %llu, \"queue_ms\": %.3f, \"run_ms\": %.3f, \"latency_ms\": %.3f, "
+          "\"uploaded_ms\": %.3f, \"lock_ms\": %.3f, \"tree_ms\": %.3f, \"start_ms\": %.3f}\n",
           (unsigned long long)j.id, j.desc.hasher.field, j.desc.log_h, j.desc.width, j.desc.log_blowup,
           j.desc.with_fri, rc, (unsigned long long)((1ull << j.desc.log_h) * j.desc.width),
-          ms(j.t_start - j.t_submit).count(), ms(done - j.t_start).count(), ms(done - j.t_submit).count());
+          ms(j.t_start - j.t_submit).count(), ms(done - j.t_start).count(), ms(done - j.t_submit).count(),
+          // stage ends, from the job's start
+          ms(j.stages.uploaded - j.t_start).count(), ms(j.stages.lock_taken - j.t_start).count(),
+          ms(j.stages.tree_built - j.t_start).count(),
+          // the job's start on the engine's clock (its first job's submission)
+          ms(j.t_start - log_epoch()).count());
   fclose(f);
 }
 
@@ -184,7 +196,7 @@ struct zkb_engine {
       int rc = pcs_job_run(job->spec, job->desc.trace, job->desc.log_h, job->desc.width,
                            job->desc.log_blowup, job->desc.alpha, job->desc.with_fri ? &prm : nullptr,
                            job->root, fri ? &fri->f : nullptr, s, &upload_mu,
-                           &compute_mu[size_class(*job)]);
+                           &compute_mu[size_class(*job)], &job->stages, streams[0]);
       std::string err = rc == ZKB_OK ? "" : zkb_last_error_message();
       ENGINE_TRACE("end job %llu rc=%d %s\n", (unsigned long long)job->id, rc, err.c_str());
       log_job(*job, rc, Clock::now());
@@ -263,6 +275,7 @@ int zkb_engine_submit(zkb_engine *e, const zkb_job_desc *desc, uint64_t *job_id)
                 (unsigned long long)job->mem_estimate, (unsigned long long)e->budget);
     job->id = e->next_id++;
     job->t_submit = Clock::now();
+    (void)log_epoch();  // the job log's clock starts at the first submission
     e->jobs[job->id] = job;
     e->queue.push_back(job);
   }
