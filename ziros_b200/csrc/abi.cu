@@ -522,18 +522,23 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
 
 }  // extern "C"
 
+thread_local zkb::JobStages *zkb::t_job_stages = nullptr;
+
 // One engine job: host trace in, root (and the FRI answers) out, device state released
 // before returning.
 int zkb::pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                      uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
                      FriProof *fri_out, cudaStream_t s, UploadGate *upload_mu, std::mutex *compute_mu,
                      JobStages *stages, cudaStream_t fri_stream) {
+  t_job_stages = stages;
   std::unique_lock<std::mutex> cl;
   if (compute_mu) cl = std::unique_lock<std::mutex>(*compute_mu, std::defer_lock);
   int rc = pcs_commit_impl(spec, nullptr, h_trace, log_h, width, log_blowup, root_out, nullptr, s,
                            alpha, fri, fri_out, upload_mu, compute_mu ? &cl : nullptr, stages, fri_stream);
   if (fri_out) fri_out->release_device();
-  if (rc == ZKB_OK) ZKB_TRY(wait_stream(s));
+  if (rc == ZKB_OK) rc = wait_stream(s);
+  if (stages) stages->released = std::chrono::steady_clock::now();
+  t_job_stages = nullptr;
   return rc;  // the compute lock (if taken) is released here, after the job's work
 }
 

@@ -4,7 +4,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -43,11 +45,16 @@ int current_context(DeviceContext **out) {
     c->device = dev;
     ZKB_CHECK_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, dev));
     // Keep freed scratch in the pool: commits of the same shape reuse it without
-    // returning memory to the driver between calls.
+    // returning memory to the driver between calls.  A block freed on one stream is reused
+    // on another only once its free has completed (or the stream already waits for it):
+    // reuse through an inserted dependency would make, e.g., one engine job's FRI phase
+    // wait for every kernel queued on another job's stream.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
       uint64_t thr = UINT64_MAX;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+      int no = 0;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
     }
     g_ctx[dev] = std::move(c);
   }
@@ -362,6 +369,47 @@ std::atomic<uint64_t> g_device_allocs{0};
 void note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
 uint64_t device_alloc_count() { return g_device_allocs.load(std::memory_order_relaxed); }
 
+// ---- large blocks: an exact-size cache in front of the stream-ordered pool
+// Repeated jobs of one shape ask for the same sizes (staged trace, LDE, tree layers, FRI
+// state).  A freed block of at least kCacheMin bytes is kept, with an event recorded on the
+// stream that freed it, and the next request of the same rounded size on the same device
+// takes it once that event has completed — work of any stream can reuse it with no
+// dependency inserted.  Without the cache, pool fragmentation made the pool grow (map and
+// clear fresh memory) in the middle of jobs, stalls of hundreds of milliseconds.  When the
+// pool runs out of memory the cached blocks go back to it and the request is retried.
+// Allocations and frees on a capturing stream bypass the cache (graph memory nodes).
+namespace {
+constexpr size_t kCacheMin = 1u << 20;
+constexpr size_t kCacheRound = 2u << 20;
+struct CachedBlock {
+  void *p;
+  cudaEvent_t freed;
+};
+std::mutex g_cache_mu;
+std::map<void *, std::pair<size_t, int>> g_cache_live;            // block -> (rounded size, device)
+std::multimap<std::pair<int, size_t>, CachedBlock> g_cache_free;   // (device, size) -> blocks
+
+bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+// Returns the cached blocks of `dev` to the pool (on s, after their frees); with
+// `completed_only`, only those whose free has completed.  Called with g_cache_mu held.
+void cache_flush(int dev, cudaStream_t s, bool completed_only) {
+  for (auto it = g_cache_free.begin(); it != g_cache_free.end();) {
+    if (it->first.first != dev || (completed_only && cudaEventQuery(it->second.freed) != cudaSuccess)) {
+      ++it;
+      continue;
+    }
+    cudaStreamWaitEvent(s, it->second.freed, 0);
+    cudaFreeAsync(it->second.p, s);
+    cudaEventDestroy(it->second.freed);
+    it = g_cache_free.erase(it);
+  }
+}
+}  // namespace
+
 int dev_alloc(void **p, size_t bytes, cudaStream_t s) {
   note_device_alloc();
   if (take_injected(g_inject_oom)) {
@@ -369,17 +417,65 @@ int dev_alloc(void **p, size_t bytes, cudaStream_t s) {
     set_error("device allocation of %zu bytes failed: out of memory (injected)", bytes);
     return ZKB_ERR_OOM;
   }
-  cudaError_t e = cudaMallocAsync(p, bytes, s);
+  const bool cached = bytes >= kCacheMin && !capturing(s);
+  const size_t rb = cached ? (bytes + kCacheRound - 1) / kCacheRound * kCacheRound : bytes;
+  int dev = 0;
+  if (cached) {
+    ZKB_CHECK_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto range = g_cache_free.equal_range({dev, rb});
+    for (auto it = range.first; it != range.second; ++it)
+      if (cudaEventQuery(it->second.freed) == cudaSuccess) {
+        *p = it->second.p;
+        cudaEventDestroy(it->second.freed);
+        g_cache_free.erase(it);
+        g_cache_live[*p] = {rb, dev};
+        return ZKB_OK;
+      }
+  }
+  cudaError_t e = cudaMallocAsync(p, rb, s);
+  if (e == cudaErrorMemoryAllocation && cached) {
+    cudaGetLastError();
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    cache_flush(dev, s, true);
+    e = cudaMallocAsync(p, rb, s);
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      cache_flush(dev, s, false);
+      e = cudaMallocAsync(p, rb, s);
+    }
+  }
   if (e != cudaSuccess) {
     *p = nullptr;
     set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? ZKB_ERR_OOM : ZKB_ERR_CUDA;
   }
+  if (cached) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    g_cache_live[*p] = {rb, dev};
+  }
   return ZKB_OK;
 }
 
 void dev_free(void *p, cudaStream_t s) {
-  if (p) cudaFreeAsync(p, s);
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto it = g_cache_live.find(p);
+    if (it != g_cache_live.end()) {
+      const std::pair<int, size_t> key{it->second.second, it->second.first};
+      g_cache_live.erase(it);
+      cudaEvent_t ev = nullptr;
+      if (!capturing(s) && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+        if (cudaEventRecord(ev, s) == cudaSuccess) {
+          g_cache_free.insert({key, CachedBlock{p, ev}});
+          return;
+        }
+        cudaEventDestroy(ev);
+      }
+    }
+  }
+  cudaFreeAsync(p, s);
 }
 
 }  // namespace zkb

@@ -173,7 +173,10 @@ class UploadGate {
 // Host times (steady clock) at which an engine job's stages ended, for the job log.
 struct JobStages {
   std::chrono::steady_clock::time_point uploaded, lock_taken, tree_built;
+  std::chrono::steady_clock::time_point fri_alloc, fri_enqueued, fri_answers, released;
 };
+// The stage record of the engine job running on this thread (null outside engine jobs).
+extern thread_local JobStages *t_job_stages;
 int pcs_job_run(const HasherSpec &spec, const void *h_trace, uint32_t log_h, uint32_t width,
                 uint32_t log_blowup, const uint32_t *alpha, const zkb_fri_params *fri, void *root_out,
                 FriProof *fri_out, cudaStream_t s, UploadGate *upload_mu = nullptr,

@@ -276,7 +276,7 @@ void FriProof::release_device() {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
-  for (void *p : owned) cudaFreeAsync(p, stream);
+  for (void *p : owned) dev_free(p, stream);
   owned.clear();
   cudaSetDevice(prev);
 }
@@ -356,6 +356,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
   void *arena = nullptr;
   ZKB_TRY(dev_alloc(&arena, off, s));
   pf->owned.push_back(arena);
+  if (t_job_stages) t_job_stages->fri_alloc = std::chrono::steady_clock::now();
   char *base = (char *)arena;
   auto cw = [&](int r) -> const uint32_t * {
     return r == 0 ? d_codeword : (const uint32_t *)(base + cw_off[r]);
@@ -420,6 +421,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
   }
 
   // ---- answers to the host: roots, final codeword, query openings
+  if (t_job_stages) t_job_stages->fri_enqueued = std::chrono::steady_clock::now();
   pf->roots.resize((size_t)rounds * 8);
   ZKB_CHECK_CUDA(cudaMemcpyAsync(pf->roots.data(), base + roots_off, (size_t)rounds * 32, cudaMemcpyDeviceToHost, s));
   pf->final_cw.resize((1ull << log_final) * 4);
@@ -457,6 +459,7 @@ int fri_commit_ext4_dev(const HasherSpec &spec, const uint32_t *d_codeword, int 
   }
   // the host tables above must outlive their (staged) uploads; the answers must be on the host
   ZKB_TRY(wait_stream(s));
+  if (t_job_stages) t_job_stages->fri_answers = std::chrono::steady_clock::now();
   return ZKB_OK;
 }
 

@@ -161,8 +161,8 @@ DeviceTree::~DeviceTree() {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
-  if (d_layers && !borrowed) cudaFreeAsync(d_layers, stream);
-  for (void *p : owned) cudaFreeAsync(p, stream);
+  if (d_layers && !borrowed) dev_free(d_layers, stream);
+  for (void *p : owned) dev_free(p, stream);
   cudaSetDevice(prev);
 }
 

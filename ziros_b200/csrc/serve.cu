@@ -83,13 +83,16 @@ void log_job(const Job &j, int rc, Clock::time_point done) {
   fprintf(f,
           "{\"job\": %llu, \"field\": %d, \"log_h\": %u, \"width\": %u, \"log_blowup\": %u, \"fri\": %d, "
           "\"status\": %d, \"cells\": %llu, \"queue_ms\": %.3f, \"run_ms\": %.3f, \"latency_ms\": %.3f, "
-          "\"uploaded_ms\": %.3f, \"lock_ms\": %.3f, \"tree_ms\": %.3f, \"start_ms\": %.3f}\n",
+          "\"uploaded_ms\": %.3f, \"lock_ms\": %.3f, \"tree_ms\": %.3f, \"fri_alloc_ms\": %.3f, "
+          "\"fri_enqueued_ms\": %.3f, \"fri_answers_ms\": %.3f, \"released_ms\": %.3f, \"start_ms\": %.3f}\n",
           (unsigned long long)j.id, j.desc.hasher.field, j.desc.log_h, j.desc.width, j.desc.log_blowup,
           j.desc.with_fri, rc, (unsigned long long)((1ull << j.desc.log_h) * j.desc.width),
           ms(j.t_start - j.t_submit).count(), ms(done - j.t_start).count(), ms(done - j.t_submit).count(),
           // stage ends, from the job's start
           ms(j.stages.uploaded - j.t_start).count(), ms(j.stages.lock_taken - j.t_start).count(),
-          ms(j.stages.tree_built - j.t_start).count(),
+          ms(j.stages.tree_built - j.t_start).count(), ms(j.stages.fri_alloc - j.t_start).count(),
+          ms(j.stages.fri_enqueued - j.t_start).count(), ms(j.stages.fri_answers - j.t_start).count(),
+          ms(j.stages.released - j.t_start).count(),
           // the job's start on the engine's clock (its first job's submission)
           ms(j.t_start - log_epoch()).count());
   fclose(f);
