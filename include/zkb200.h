@@ -90,6 +90,11 @@ ZKB_API int zkb_debug_inject_fault(int kind, int count);
  * made in this process.  Tests read it around a call to check that the call allocated
  * nothing.  No counterpart in the reference. */
 ZKB_API uint64_t zkb_debug_device_allocations(void);
+/* Device memory the library keeps for reuse on the current device — freed blocks it caches
+ * for allocations of the same size, and the stream-ordered pool's unused memory — goes
+ * back to the device, e.g. before a large cudaMalloc of the caller's.  zkb_batch_create
+ * does this itself.  No counterpart in the reference. */
+ZKB_API int zkb_release_cached_memory(void);
 
 /* Kernel timing.  zkb_profile_start() enables per-launch CUDA events (recorded on
  * the stream each kernel is launched on) and clears earlier records;
@@ -507,7 +512,10 @@ typedef struct {
 } zkb_batch_shape;
 typedef struct {
   uint32_t log_blowup;   /* 1..4 */
-  int use_graph;         /* 1: one CUDA graph per run; 0: the same launches on streams */
+  int use_graph;         /* 1: one CUDA graph per run; 0: the same launches on streams;
+                            2: one persistent kernel per run, fed by a device work queue and
+                            captured in a CUDA graph (BabyBear, width-16 hasher, widths that
+                            are multiples of 8, 2^(log_h + log_blowup) <= 2^25) */
   uint32_t branches;     /* concurrent LDE branches (1..8); 0 = tuned/default */
   int autotune;          /* time kernel-shape candidates at creation */
   const char *tune_cache;/* JSON-lines file read (and rewritten after tuning); NULL = none */
@@ -538,6 +546,29 @@ ZKB_API int zkb_batch_info(const zkb_batch *batch, zkb_batch_info_t *info);
 /* Kernel shapes chosen for trace i's LDE (0 = default). */
 ZKB_API int zkb_batch_lde_tune(const zkb_batch *batch, size_t i, int *kmax, uint32_t *c_pass,
                                uint32_t *c_fused);
+/* Merkle-level fusion of a persistent plan (use_graph = 2): the levels above the leaves
+ * that each leaf-hash tile of 256 rows also computes in shared memory (0..8), and the
+ * levels each compression tile computes (1..8).  Rebuilds the work queue and the graph;
+ * the autotuner sets them at creation.  No counterpart in the reference. */
+ZKB_API int zkb_batch_set_merkle_fusion(zkb_batch *batch, uint32_t leaf_levels, uint32_t comp_levels);
+typedef struct {
+  uint32_t items;        /* work items in the queue */
+  uint32_t steps;        /* dependency steps (one counter each) */
+  uint32_t stages;
+  uint32_t grid;         /* blocks of the persistent kernel */
+  uint32_t leaf_levels, comp_levels;
+} zkb_batch_queue_info_t;
+ZKB_API int zkb_batch_queue_info(const zkb_batch *batch, zkb_batch_queue_info_t *info);
+/* One profiled run of a persistent plan (waits for it): busy_ms[4] = the blocks' summed
+ * busy time on NTT passes, fused LDE middles, leaf hashing and compression items; span_ms
+ * = first item start to last item end (global timer).  No counterpart in the reference. */
+ZKB_API int zkb_batch_profile(zkb_batch *batch, void *stream, double *busy_ms, double *span_ms);
+/* Test hook of a persistent plan: one run (not the graph) in which a work item waits on a
+ * counter that nothing bumps, polling at most spin_limit times (1..2^24) before it gives up;
+ * the kernel then records the item, every block leaves the queue, and the next
+ * zkb_batch_roots returns ZKB_ERR_TIMEOUT.  The run's results are invalid; the next
+ * zkb_batch_run recomputes everything.  No device fault is involved. */
+ZKB_API int zkb_debug_batch_stalled_run(zkb_batch *batch, uint64_t spin_limit, void *stream);
 ZKB_API void zkb_batch_free(zkb_batch *batch);
 
 #ifdef __cplusplus

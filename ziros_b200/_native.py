@@ -101,6 +101,11 @@ class BatchInfo(C.Structure):
                 ("tune_ms", C.c_double)]
 
 
+class BatchQueueInfo(C.Structure):
+    _fields_ = [("items", C.c_uint32), ("steps", C.c_uint32), ("stages", C.c_uint32), ("grid", C.c_uint32),
+                ("leaf_levels", C.c_uint32), ("comp_levels", C.c_uint32)]
+
+
 class EngineStats(C.Structure):
     _fields_ = [("queued", C.c_uint64), ("completed", C.c_uint64), ("hbm_budget", C.c_uint64),
                 ("hbm_in_use", C.c_uint64), ("hbm_peak", C.c_uint64)]
@@ -179,7 +184,12 @@ SIGNATURES = {
     "zkb_circuit_open": (_I, [C.c_char_p, _SZ]),
     "zkb_circuit_reset": (None, []),
     "zkb_debug_inject_fault": (_I, [_I, _I]),
+    "zkb_batch_set_merkle_fusion": (_I, [_P, _U32, _U32]),
+    "zkb_batch_queue_info": (_I, [_P, _P]),
+    "zkb_batch_profile": (_I, [_P, _P, _P, _P]),
+    "zkb_debug_batch_stalled_run": (_I, [_P, _U64, _P]),
     "zkb_debug_device_allocations": (_U64, []),
+    "zkb_release_cached_memory": (_I, []),
     "zkb_engine_cancel": (_I, [_P, _U64]),
     "zkb_mmcs_verify_batch": (_I, [_P, _P, _P, _P, _SZ, _U64, _P, _P, _SZ]),
     "zkb_challenger_create": (_I, [_P, _P]),
@@ -255,6 +265,11 @@ def inject_fault(kind: int, count: int = 1) -> None:
 def device_allocations() -> int:
     """Device allocations the library has made in this process (pool or cudaMalloc)."""
     return int(load().zkb_debug_device_allocations())
+
+
+def release_cached_memory() -> None:
+    """Returns the library's cached device blocks and the pool's unused memory to the device."""
+    check(load().zkb_release_cached_memory())
 
 
 def last_error() -> str:

@@ -794,12 +794,14 @@ class Challenger:
 class BatchCommit:
     """Many traces of uneven height and width committed by one plan (zkb_batch_*): one
     device arena, tables built once, kernel shapes autotuned (JSON-lines cache), and one
-    CUDA graph per run.  Every root equals the trace's plain commitment
-    (CudaTwoAdicPcs.commit)."""
+    CUDA graph per run — of ordinary kernels, or with persistent=True of ONE persistent
+    kernel fed by a device work queue (BabyBear, widths that are multiples of 8), whose
+    Merkle-level fusion the autotuner also chooses.  Every root equals the trace's plain
+    commitment (CudaTwoAdicPcs.commit)."""
 
     def __init__(self, shapes: Sequence[Tuple[int, int]], field: int = BABYBEAR, seed: int = 42,
                  log_blowup: int = 1, p2_width: int = 16, use_graph: bool = True, branches: int = 0,
-                 autotune: bool = True, tune_cache: Optional[str] = None):
+                 autotune: bool = True, tune_cache: Optional[str] = None, persistent: bool = False):
         lib = N.load()
         self.field = field
         self.shapes = [(int(h), int(w)) for h, w in shapes]
@@ -810,7 +812,7 @@ class BatchCommit:
         self.digest_elems = 8 if p2_width == 16 else 4
         self.hasher = N.Hasher(field, p2_width, seed)
         arr = (N.BatchShape * len(self.shapes))(*[N.BatchShape(h.bit_length() - 1, w) for h, w in self.shapes])
-        opt = N.BatchOptions(log_blowup, int(use_graph), branches, int(autotune),
+        opt = N.BatchOptions(log_blowup, 2 if persistent else int(use_graph), branches, int(autotune),
                              tune_cache.encode() if tune_cache else None)
         self._h = C.c_void_p()
         N.check(lib.zkb_batch_create(C.byref(self.hasher), arr, len(self.shapes), C.byref(opt), C.byref(self._h)))
@@ -837,6 +839,29 @@ class BatchCommit:
 
     def run(self, stream=None) -> None:
         N.check(N.load().zkb_batch_run(self._h, stream))
+
+    def set_merkle_fusion(self, leaf_levels: int, comp_levels: int) -> None:
+        """Persistent plans: Merkle levels the leaf tile computes above the leaves (0..8)
+        and levels per compression tile (1..8)."""
+        N.check(N.load().zkb_batch_set_merkle_fusion(self._h, leaf_levels, comp_levels))
+
+    def queue_info(self) -> dict:
+        q = N.BatchQueueInfo()
+        N.check(N.load().zkb_batch_queue_info(self._h, C.byref(q)))
+        return {k: int(getattr(q, k)) for k, _ in N.BatchQueueInfo._fields_}
+
+    def profile(self, stream=None) -> dict:
+        """One profiled run of a persistent plan: summed block-busy ms by item kind, span ms."""
+        busy = (C.c_double * 4)()
+        span = C.c_double()
+        N.check(N.load().zkb_batch_profile(self._h, stream, busy, C.byref(span)))
+        return {"pass_ms": busy[0], "fused_ms": busy[1], "leaf_ms": busy[2], "compress_ms": busy[3],
+                "span_ms": span.value}
+
+    def debug_stalled_run(self, spin_limit: int, stream=None) -> None:
+        """One run whose work queue holds an item waiting on a counter nothing bumps: the
+        kernel gives up after spin_limit polls and roots() then raises ZKB_ERR_TIMEOUT."""
+        N.check(N.load().zkb_debug_batch_stalled_run(self._h, spin_limit, stream))
 
     def roots(self, stream=None) -> np.ndarray:
         out = np.zeros((len(self), self.digest_elems), dtype=dtype_of(self.field))

@@ -167,6 +167,13 @@ int zkb_debug_inject_fault(int kind, int count) {
 
 uint64_t zkb_debug_device_allocations(void) { return device_alloc_count(); }
 
+int zkb_release_cached_memory(void) {
+  clear_error();
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return ZKB_OK;
+  return release_cached_memory();
+}
+
 int zkb_set_device(int device) {
   clear_error();
   ZKB_CHECK_CUDA(cudaSetDevice(device));

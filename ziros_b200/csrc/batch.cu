@@ -12,6 +12,13 @@
 //           that level
 //        -> one launch gathering the roots
 //
+// With use_graph = 2 (BabyBear, widths that are multiples of 8) a run is instead ONE
+// persistent kernel fed by a device work queue (persist.cu), captured in the graph: every
+// trace's NTT passes, leaf hashing and compression levels are items that the kernel's
+// blocks claim in order, each waiting (bounded) for the step it depends on; the
+// autotuner then also chooses the Merkle-level fusion (levels computed in shared memory by
+// the tile that made the level below).
+//
 // Every trace gets exactly the p3 MerkleTree of its own LDE (power-of-two heights: no
 // padding, no injection), so each root equals the plain per-trace commitment
 // (TwoAdicFriPcs::commit over one matrix, vendor/p3-merkle-tree-gpu/src/merkle_tree.rs:84-151).
@@ -31,6 +38,7 @@
 #include "common.cuh"
 #include "engine.cuh"
 #include "multitree.cuh"
+#include "persist.cuh"
 #include "poseidon2.cuh"
 
 namespace zkb {
@@ -126,6 +134,13 @@ struct zkb_batch {
   uint32_t branches = 1;
   std::vector<std::vector<int>> branch_traces;
   bool use_graph = true;
+  bool persistent = false;             // one persistent kernel per run (use_graph = 2)
+  std::unique_ptr<PersistPlan> persist;
+  void *d_coef_all = nullptr;          // persistent form: coefficient scratch slots
+  std::vector<uint32_t *> coef_of;     // per trace: its slot
+  std::vector<int> slot_prev, round_of, queue_order;
+  uint32_t coef_slots = 0;
+  MerkleFusion fusion{3, 4};
   bool tuned_from_cache = false;
   double tune_ms = 0;
   // execution
@@ -146,6 +161,8 @@ struct zkb_batch {
     if (s_main) cudaStreamSynchronize(s_main);
     trees.clear();
     if (!d_coef.empty()) cudaFree(d_coef[0]);
+    persist.reset();
+    if (d_coef_all) cudaFree(d_coef_all);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     for (auto e : ev_br) cudaEventDestroy(e);
@@ -187,7 +204,35 @@ struct zkb_batch {
     return hash_all<Goldilocks, 12>(p_gl12, threads, s);
   }
 
+  // The persistent form's plan over the current kernel shapes and Merkle fusion.
+  int build_persist() {
+    // the plan's traces in queue order (largest first); slot_prev refers to that order
+    std::vector<PersistTrace> tr(shapes.size());
+    for (size_t k = 0; k < shapes.size(); k++) {
+      const size_t i = (size_t)queue_order[k];
+      tr[k].slot_prev = slot_prev[k];
+      tr[k].round = round_of[k];
+      tr[k].in = (const uint32_t *)d_in[i];
+      tr[k].coef = coef_of[i];
+      tr[k].lde = (uint32_t *)d_lde[i];
+      tr[k].layers = (uint32_t *)d_layers[i];
+      tr[k].root = (uint32_t *)d_roots + i * 8;
+      tr[k].log_h = (int)shapes[i].log_h;
+      tr[k].width = shapes[i].width;
+      tr[k].kmax = std::min(tune[i].kmax ? tune[i].kmax : 9, 9);
+    }
+    auto plan = std::make_unique<PersistPlan>();
+    ZKB_TRY(plan->build(tr, (int)log_b, p_bb16, fusion, s_main));
+    persist = std::move(plan);
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    return ZKB_OK;
+  }
+
   int enqueue(cudaStream_t origin) {
+    if (persistent) return persist->enqueue(origin);
     const uint32_t nb = (uint32_t)branch_traces.size();
     ZKB_CHECK_CUDA(cudaEventRecord(ev_fork, origin));
     for (uint32_t b = 0; b < nb; b++) {
@@ -317,7 +362,8 @@ struct zkb_batch {
   }
 
   int tune_lde(TuneCache &cache, bool autotune) {
-    const int kdef = spec.field == FIELD_BABYBEAR ? 10 : 7;  // the default plans' largest pass
+    // the default plans' largest pass (the persistent kernel's tiles take at most 9 bits)
+    const int kdef = spec.field == FIELD_BABYBEAR ? (persistent ? 9 : 10) : 7;
     std::vector<std::pair<std::string, LdeTune>> done;
     for (size_t i = 0; i < shapes.size(); i++) {
       const std::string key = lde_key(i);
@@ -404,6 +450,42 @@ struct zkb_batch {
     return k;
   }
 
+  // Persistent form: the Merkle-level fusion (levels above the leaves in the leaf tile,
+  // levels per compression tile), timed over whole runs, cached per batch signature.
+  int tune_fusion(TuneCache &cache, bool autotune) {
+    const std::string key = batch_key("fusion");
+    long lv = 0, cv = 0;
+    if (const std::string *ln = cache.find(key); ln && TuneCache::field(*ln, "leaf_levels", &lv) &&
+                                                 TuneCache::field(*ln, "comp_levels", &cv) && lv >= 0 &&
+                                                 lv <= 8 && cv >= 1 && cv <= 8) {
+      fusion = MerkleFusion{(uint32_t)lv, (uint32_t)cv};
+      tuned_from_cache = true;
+      return build_persist();
+    }
+    if (!autotune) return build_persist();
+    float best = 1e30f;
+    MerkleFusion bf = fusion;
+    for (uint32_t l : {0u, 2u, 4u, 8u})
+      for (uint32_t c : {1u, 4u, 8u}) {
+        fusion = MerkleFusion{l, c};
+        ZKB_TRY(build_persist());
+        float ms = 0;
+        ZKB_TRY(time_ms([&] { return persist->enqueue(s_main); }, 2, &ms));
+        ZKB_TRY(persist->check(s_main));
+        if (ms < best) {
+          best = ms;
+          bf = fusion;
+        }
+      }
+    fusion = bf;
+    ZKB_TRY(build_persist());
+    char ln[256];
+    snprintf(ln, sizeof ln, "{\"key\": \"%s\", \"leaf_levels\": %u, \"comp_levels\": %u, \"us\": %d}",
+             key.c_str(), fusion.leaf_levels, fusion.comp_levels, (int)(best * 1000));
+    cache.put(key, ln);
+    return ZKB_OK;
+  }
+
   int tune_leaf_and_branches(TuneCache &cache, bool autotune, uint32_t fixed_branches) {
     const std::string lk = batch_key("leaf"), bk = batch_key("branches");
     long v = 0;
@@ -472,6 +554,8 @@ constexpr uint32_t MAX_BRANCHES = 8;
 
 int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   const size_t n = b->shapes.size();
+  // the arena is one cudaMalloc: memory the library keeps for reuse goes back first
+  ZKB_TRY(release_cached_memory());
   const int OUT = b->out;
   const size_t es = b->es;
   const uint32_t nb_max = std::min<uint32_t>(MAX_BRANCHES, (uint32_t)n);
@@ -518,6 +602,47 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
     b->d_layers[i] = base + layers_base + lay_off[i] * OUT * es;
   }
   b->d_roots = base + roots_off;
+  if (b->persistent) {
+    // Coefficient scratch of the inverse passes in S slots shared round-robin by the traces
+    // taken largest first: trace k of that order uses slot k % S after trace k - S, whose
+    // fused step (the scratch's last reader) it waits for; the queue runs the traces in
+    // rounds of S.  S is as large as free memory allows (2 GiB kept free), at most 16, or
+    // at most ZKB_PERSIST_SLOTS when that is set.
+    std::vector<int> ord(n);
+    std::iota(ord.begin(), ord.end(), 0);
+    auto cells = [&](int i) { return (uint64_t)b->shapes[i].width << b->shapes[i].log_h; };
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cells(x) > cells(y); });
+    ZKB_CHECK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    uint32_t S = 0, s_max = 16;
+    if (const char *v = getenv("ZKB_PERSIST_SLOTS"); v && atoi(v) >= 1) s_max = std::min<uint32_t>(16, atoi(v));
+    uint64_t coef_total = 0;
+    while (S < n && S < s_max) {
+      const uint64_t add = align256(cells(ord[S]) * es);
+      if (coef_total + add + (2ull << 30) > free_b) break;
+      coef_total += add;
+      S++;
+    }
+    ZKB_REQUIRE(S >= 1, "the persistent form needs %llu more bytes of device memory, %llu free",
+                (unsigned long long)align256(cells(ord[0]) * es), (unsigned long long)free_b);
+    note_device_alloc();
+    ZKB_CHECK_CUDA(cudaMalloc(&b->d_coef_all, coef_total));
+    std::vector<uint32_t *> slot(S);
+    uint64_t o = 0;
+    for (uint32_t k = 0; k < S; k++) {
+      slot[k] = (uint32_t *)((char *)b->d_coef_all + o);
+      o += align256(cells(ord[k]) * es);
+    }
+    b->coef_slots = S;
+    b->coef_of.assign(n, nullptr);
+    b->queue_order = ord;
+    b->slot_prev.assign(n, -1);
+    b->round_of.assign(n, 0);
+    for (size_t k = 0; k < n; k++) {
+      b->coef_of[ord[k]] = slot[k % S];
+      b->slot_prev[k] = k >= S ? (int)(k - S) : -1;
+      b->round_of[k] = (int)(k / S);
+    }
+  }
 
   // ---- job tables
   std::vector<const void *> data(n);
@@ -563,7 +688,9 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   // read (some depend on the pass split), so nothing is built inside a graph capture
   for (size_t i = 0; i < n && rc == ZKB_OK; i++) rc = b->lde_one(i, b->s_main, &b->tune[i]);
   if (rc == ZKB_OK) rc = wait_stream(b->s_main);
-  if (rc == ZKB_OK) rc = b->tune_leaf_and_branches(cache, opt.autotune != 0, std::min(opt.branches, nb_max));
+  if (rc == ZKB_OK)
+    rc = b->persistent ? b->tune_fusion(cache, opt.autotune != 0)
+                       : b->tune_leaf_and_branches(cache, opt.autotune != 0, std::min(opt.branches, nb_max));
   cudaEventRecord(t1, b->s_main);
   cudaEventSynchronize(t1);
   float ms = 0;
@@ -628,6 +755,16 @@ int zkb_batch_create(const zkb_hasher *hasher, const zkb_batch_shape *shapes, si
   b->es = field_elem_bytes(hasher->field);
   b->out = b->spec.out;
   b->use_graph = opt->use_graph != 0;
+  b->persistent = opt->use_graph == 2;
+  if (b->persistent) {
+    ZKB_REQUIRE(hasher->field == ZKB_FIELD_BABYBEAR && hasher->width == 16,
+                "the persistent form commits BabyBear traces with the width-16 hasher");
+    for (size_t i = 0; i < n; i++)
+      ZKB_REQUIRE(shapes[i].width % 8 == 0 && shapes[i].log_h >= 1 && shapes[i].log_h + opt->log_blowup <= 25,
+                  "trace %zu: the persistent form takes widths that are multiples of 8 and 2^1..2^%u rows (got "
+                  "2^%u x %u)",
+                  i, 25 - opt->log_blowup, shapes[i].log_h, shapes[i].width);
+  }
   bool ok;
   if (b->spec.field == FIELD_BABYBEAR)
     ok = build_p2_params<BabyBear, 16>(b->spec, &b->p_bb16);
@@ -673,6 +810,7 @@ int zkb_batch_roots(zkb_batch *b, void *roots_out, void *stream) {
   ZKB_REQUIRE(b && roots_out, "null arguments");
   ZKB_CHECK_CUDA(cudaSetDevice(b->device));
   cudaStream_t s = resolve_stream(stream);
+  if (b->persistent) ZKB_TRY(b->persist->check(s));  // a work item's wait gave up: no roots
   ZKB_CHECK_CUDA(cudaMemcpyAsync(roots_out, b->d_roots, b->shapes.size() * b->out * b->es,
                                  cudaMemcpyDeviceToHost, s));
   ZKB_TRY(wait_stream(s));
@@ -691,9 +829,9 @@ int zkb_batch_info(const zkb_batch *b, zkb_batch_info_t *info) {
   ZKB_REQUIRE(b && info, "null arguments");
   info->device_bytes = b->arena_bytes;
   info->kernels_per_run = b->use_graph ? b->kernels_per_run : 0;
-  info->branches = b->branches;
+  info->branches = b->persistent ? 0 : b->branches;
   info->leaf_threads = b->leaf_threads;
-  info->use_graph = b->use_graph ? 1 : 0;
+  info->use_graph = b->persistent ? 2 : b->use_graph ? 1 : 0;
   info->tuned_from_cache = b->tuned_from_cache ? 1 : 0;
   info->tune_ms = b->tune_ms;
   return ZKB_OK;
@@ -706,6 +844,52 @@ int zkb_batch_lde_tune(const zkb_batch *b, size_t i, int *kmax, uint32_t *c_pass
   *c_pass = b->tune[i].c_pass;
   *c_fused = b->tune[i].c_fused;
   return ZKB_OK;
+}
+
+int zkb_batch_set_merkle_fusion(zkb_batch *b, uint32_t leaf_levels, uint32_t comp_levels) {
+  clear_error();
+  ZKB_REQUIRE(b != nullptr, "null batch");
+  ZKB_REQUIRE(b->persistent, "Merkle-level fusion applies to the persistent form (use_graph = 2)");
+  ZKB_REQUIRE(leaf_levels <= 8 && comp_levels >= 1 && comp_levels <= 8,
+              "leaf levels %u (0..8), compression levels %u (1..8)", leaf_levels, comp_levels);
+  ZKB_CHECK_CUDA(cudaSetDevice(b->device));
+  ZKB_TRY(wait_stream(b->s_main));
+  b->fusion = MerkleFusion{leaf_levels, comp_levels};
+  ZKB_TRY(b->build_persist());
+  if (b->use_graph) ZKB_TRY(b->capture());
+  return ZKB_OK;
+}
+
+int zkb_batch_queue_info(const zkb_batch *b, zkb_batch_queue_info_t *info) {
+  clear_error();
+  ZKB_REQUIRE(b && info, "null arguments");
+  ZKB_REQUIRE(b->persistent && b->persist, "not a persistent plan");
+  const PersistStats st = b->persist->stats();
+  info->items = st.items;
+  info->steps = st.steps;
+  info->stages = st.stages;
+  info->grid = st.grid;
+  info->leaf_levels = b->fusion.leaf_levels;
+  info->comp_levels = b->fusion.comp_levels;
+  return ZKB_OK;
+}
+
+int zkb_batch_profile(zkb_batch *b, void *stream, double *busy_ms, double *span_ms) {
+  clear_error();
+  ZKB_REQUIRE(b && busy_ms && span_ms, "null arguments");
+  ZKB_REQUIRE(b->persistent && b->persist, "not a persistent plan");
+  ZKB_CHECK_CUDA(cudaSetDevice(b->device));
+  return b->persist->profile(resolve_stream(stream), busy_ms, span_ms);
+}
+
+int zkb_debug_batch_stalled_run(zkb_batch *b, uint64_t spin_limit, void *stream) {
+  clear_error();
+  ZKB_REQUIRE(b != nullptr, "null batch");
+  ZKB_REQUIRE(b->persistent && b->persist, "not a persistent plan");
+  ZKB_REQUIRE(spin_limit >= 1 && spin_limit <= (1ull << 24), "spin limit %llu (1..2^24)",
+              (unsigned long long)spin_limit);
+  ZKB_CHECK_CUDA(cudaSetDevice(b->device));
+  return b->persist->enqueue_stalled(resolve_stream(stream), spin_limit);
 }
 
 void zkb_batch_free(zkb_batch *b) { delete b; }

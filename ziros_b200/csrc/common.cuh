@@ -78,6 +78,9 @@ int dev_alloc(void **p, size_t bytes, cudaStream_t s);
 // zkb_debug_device_allocations() reads the count.
 void note_device_alloc();
 uint64_t device_alloc_count();
+// Returns the cached blocks of the current device to the pool and trims the pool's unused
+// memory back to the device (for allocations outside the pool, e.g. a batch plan's arena).
+int release_cached_memory();
 // Host wait on a stream with the watchdog deadline (ZKB_WATCHDOG_MS, default 120 s, 0 =
 // none); a device error or an expired deadline opens the circuit.
 int wait_stream(cudaStream_t s);

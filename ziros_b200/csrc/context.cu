@@ -373,8 +373,8 @@ uint64_t device_alloc_count() { return g_device_allocs.load(std::memory_order_re
 // Repeated jobs of one shape ask for the same sizes (staged trace, LDE, tree layers, FRI
 // state).  A freed block of at least kCacheMin bytes is kept, with an event recorded on the
 // stream that freed it, and the next request of the same rounded size on the same device
-// takes it once that event has completed — work of any stream can reuse it with no
-// dependency inserted.  Without the cache, pool fragmentation made the pool grow (map and
+// takes it: on the stream that freed it at once (stream order), on any other stream once
+// that event has completed — no dependency on another stream's queued work is inserted.  Without the cache, pool fragmentation made the pool grow (map and
 // clear fresh memory) in the middle of jobs, stalls of hundreds of milliseconds.  When the
 // pool runs out of memory the cached blocks go back to it and the request is retried.
 // Allocations and frees on a capturing stream bypass the cache (graph memory nodes).
@@ -384,6 +384,7 @@ constexpr size_t kCacheRound = 2u << 20;
 struct CachedBlock {
   void *p;
   cudaEvent_t freed;
+  cudaStream_t stream;  // the stream that freed it
 };
 std::mutex g_cache_mu;
 std::map<void *, std::pair<size_t, int>> g_cache_live;            // block -> (rounded size, device)
@@ -423,15 +424,26 @@ int dev_alloc(void **p, size_t bytes, cudaStream_t s) {
   if (cached) {
     ZKB_CHECK_CUDA(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(g_cache_mu);
+    // a block freed on this stream is ordered before this use by the stream itself (the
+    // wait on its event costs nothing and stays correct if the handle was recycled); one
+    // freed on another stream only once its free has completed
     auto range = g_cache_free.equal_range({dev, rb});
-    for (auto it = range.first; it != range.second; ++it)
-      if (cudaEventQuery(it->second.freed) == cudaSuccess) {
-        *p = it->second.p;
-        cudaEventDestroy(it->second.freed);
-        g_cache_free.erase(it);
-        g_cache_live[*p] = {rb, dev};
-        return ZKB_OK;
+    auto pick = range.second;
+    for (auto it = range.first; it != range.second; ++it) {
+      if (it->second.stream == s) {
+        pick = it;
+        break;
       }
+      if (pick == range.second && cudaEventQuery(it->second.freed) == cudaSuccess) pick = it;
+    }
+    if (pick != range.second) {
+      *p = pick->second.p;
+      if (pick->second.stream == s) cudaStreamWaitEvent(s, pick->second.freed, 0);
+      cudaEventDestroy(pick->second.freed);
+      g_cache_free.erase(pick);
+      g_cache_live[*p] = {rb, dev};
+      return ZKB_OK;
+    }
   }
   cudaError_t e = cudaMallocAsync(p, rb, s);
   if (e == cudaErrorMemoryAllocation && cached) {
@@ -457,6 +469,23 @@ int dev_alloc(void **p, size_t bytes, cudaStream_t s) {
   return ZKB_OK;
 }
 
+int release_cached_memory() {
+  int dev = 0;
+  ZKB_CHECK_CUDA(cudaGetDevice(&dev));
+  cudaStream_t s = nullptr;
+  ZKB_CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    cache_flush(dev, s, false);
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  ZKB_CHECK_CUDA(e);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) ZKB_CHECK_CUDA(cudaMemPoolTrimTo(pool, 0));
+  return ZKB_OK;
+}
+
 void dev_free(void *p, cudaStream_t s) {
   if (!p) return;
   {
@@ -468,7 +497,7 @@ void dev_free(void *p, cudaStream_t s) {
       cudaEvent_t ev = nullptr;
       if (!capturing(s) && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
         if (cudaEventRecord(ev, s) == cudaSuccess) {
-          g_cache_free.insert({key, CachedBlock{p, ev}});
+          g_cache_free.insert({key, CachedBlock{p, ev, s}});
           return;
         }
         cudaEventDestroy(ev);

@@ -660,6 +660,19 @@ int ntt_dft_into(typename F::T *d, int log_h, uint32_t width, bool inverse, type
 template int ntt_dft_into<BabyBear>(uint32_t *, int, uint32_t, bool, uint32_t *, uint32_t *, cudaStream_t);
 template int ntt_dft_into<Goldilocks>(uint64_t *, int, uint32_t, bool, uint64_t *, uint64_t *, cudaStream_t);
 
+void small_twiddles_bb(bool inverse, SmallTw<BabyBear> *out) { *out = small_twiddles<BabyBear>(inverse); }
+
+int lde_plan_babybear(int log_h, int log_b, int kmax, LdePlanBB *out, cudaStream_t s) {
+  ZKB_REQUIRE(log_h >= 1 && log_h + log_b <= BabyBear::TWO_ADICITY, "LDE of 2^%d rows x2^%d", log_h, log_b);
+  out->ks = plan_passes(log_h, kmax);
+  const uint32_t *ctab;
+  ZKB_TRY(get_coset_table<BabyBear>(log_h, log_b, BabyBear::GENERATOR, &ctab, s));
+  ZKB_TRY(get_twiddles<BabyBear>(log_h, true, &out->itw, s));
+  ZKB_TRY(get_twiddles<BabyBear>(log_h, false, &out->ftw, s));
+  return get_fused_tables<BabyBear>(log_h, log_b, BabyBear::GENERATOR, out->ks.back(), ctab, out->ftw,
+                                    &out->ctab_t, &out->ftw_t, s);
+}
+
 template int get_twiddles<BabyBear>(int, bool, const uint32_t **, cudaStream_t);
 template int get_twiddles<Goldilocks>(int, bool, const uint64_t **, cudaStream_t);
 template int ntt_dft_dev<BabyBear>(uint32_t *, int, uint32_t, bool, cudaStream_t);

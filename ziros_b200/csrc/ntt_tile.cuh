@@ -2,8 +2,11 @@
 // functions: the standalone kernels of ntt.cu run one tile per block, the persistent
 // batch kernel (persist.cu) runs them as work items.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <type_traits>
 #include <utility>
+#include <vector>
 
 #include "field.cuh"
 
@@ -397,5 +400,18 @@ constexpr size_t fused_tile_smem() {
   return (size_t)PassSmem<LR2, C>::STRIDE * (1 << LR1) * sizeof(typename F::T) +
          (size_t)(2u * ((1u << LR2) * ((1u << LR1) + 1)) + (2u << (LR1 + LR2))) * sizeof(TwS<F>);
 }
+
+// ---- host side, for the persistent batch kernel (defined in ntt.cu)
+// The register-DIF constants (w_64 powers and Shoup quotients) of either direction.
+void small_twiddles_bb(bool inverse, SmallTw<BabyBear> *out);
+// The pass split and the device tables of one BabyBear coset LDE (shift = the field
+// generator, rows bit-reversed), as ntt_lde_dev runs it with passes of at most kmax bits:
+// ks = pass bits top first (the last is the fused kernel's); the tables are built on s
+// when missing (not inside a graph capture).
+struct LdePlanBB {
+  std::vector<int> ks;
+  const uint32_t *itw = nullptr, *ftw = nullptr, *ctab_t = nullptr, *ftw_t = nullptr;
+};
+int lde_plan_babybear(int log_h, int log_b, int kmax, LdePlanBB *out, cudaStream_t s);
 
 }  // namespace zkb
