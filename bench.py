@@ -58,6 +58,9 @@ WORKLOADS = {
     # batched form: 64 traces, log2 rows uniform in [12, 22], widths uniform in {8, ..., 256}
     "batch64_babybear": dict(kind="batch", field=0, n=64, log_h_lo=12, log_h_hi=22, w_step=8, w_hi=256,
                              log_blowup=1, p2w=16, seed=4, width=128, log_h=22),
+    # many small traces (launch-bound as plain calls): 256 traces, log2 rows in [8, 14], widths {8..64}
+    "batch256_small_babybear": dict(kind="batch", field=0, n=256, log_h_lo=8, log_h_hi=14, w_step=8, w_hi=64,
+                                    log_blowup=1, p2w=16, seed=9, width=36, log_h=14),
 }
 DEFAULT_WORKLOAD = "babybear_2^22x256_b2"
 P2_SEED = 42
@@ -717,7 +720,41 @@ def run_batch(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     for _ in range(args.steps):
         e2e_step()
     t_e2e = max_over_ranks(time.perf_counter() - t0)
-    # the plain path end to end: 64 host-pointer commits
+    batch.close()  # the persistent plan below needs the memory
+    del batch
+
+    # ---- the persistent form: ONE kernel per run fed by a device work queue (autotuned
+    # Merkle-level fusion), on traces generated straight into its input buffers
+    pers = None
+    if field == 0 and p2w == 16 and all(w % 8 == 0 for _, w in shapes):
+        N.release_cached_memory()
+        t0 = time.perf_counter()
+        pb = Z.BatchCommit(shapes, field=field, seed=P2_SEED, log_blowup=lb, p2_width=p2w, persistent=True,
+                           autotune=True)
+        pcreate_s = time.perf_counter() - t0
+        for i, (h, w) in enumerate(shapes):
+            t = fill_uniform(torch, field, (h, w), TRACE_SEED + i, dev)
+            pb.copy_in(i, t)
+            del t
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        for _ in range(max(args.warmup, 1)):
+            pb.run(sp)
+        assert (pb.roots(sp) == plain_roots).all(), "persistent-form roots differ from the plain commits"
+        t_pers = timed(lambda: pb.run(sp), args.steps)
+        assert (pb.roots(sp) == plain_roots).all()
+        prof = pb.profile(sp)
+        q = pb.queue_info()
+        pers = {"value": cells * args.steps * world / t_pers, "ms_per_step": 1e3 * t_pers / args.steps,
+                "vs_graph": t_batch / t_pers, "vs_plain": t_plain / t_pers, "work_queue": q,
+                "plan_create_s": pcreate_s, "tune_ms": pb.info()["tune_ms"],
+                "profile_block_ms": {k: round(v / (q["grid"] if k != "span_ms" else 1), 2) for k, v in prof.items()},
+                "path": "one persistent kernel per run (device work queue of NTT / leaf-hash / compression tiles, "
+                        "bounded waits on per-step counters) captured in a CUDA graph"}
+        pb.close()
+        del pb
+        N.release_cached_memory()
+    # the plain path end to end: one host-pointer commit per trace
     pcs = Z.CudaTwoAdicPcs(field, P2_SEED, lb, p2w)
     r = np.zeros(digest, dtype=dt)
     pcs.commit_ptr(pinned.data_ptr(), shapes[0][0], shapes[0][1], want_tree=False, root=r)
@@ -764,14 +801,15 @@ def run_batch(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
                    "plan_create_s": create_s, "tune_ms": info["tune_ms"]},
         "plain": {"value": plain, "ms_per_step": 1e3 * t_plain / args.steps,
                   "launches_per_step": plain_launches / args.steps,
-                  "path": "64 x zkb_pcs_commit_dev on the same device-resident traces"},
+                  "path": f"{len(shapes)} x zkb_pcs_commit_dev on the same device-resident traces"},
         "batched_vs_plain": value / plain,
+        "persistent": pers,
         "e2e": {"value": cells * args.steps * world / t_e2e, "unit": "cells/s",
                 "h2d_bytes_per_step": cells * esize, "d2h_bytes_per_step": len(shapes) * digest * esize,
                 "ms_per_step": 1e3 * t_e2e / args.steps,
-                "path": "zkb_batch_copy_in (pinned) x64 + zkb_batch_run + zkb_batch_roots",
+                "path": f"zkb_batch_copy_in (pinned) x{len(shapes)} + zkb_batch_run + zkb_batch_roots",
                 "plain_value": cells * args.steps * world / t_e2e_plain,
-                "plain_path": "64 x zkb_pcs_commit from pinned host memory"},
+                "plain_path": f"{len(shapes)} x zkb_pcs_commit from pinned host memory"},
         "roofline": {"kernel": "whole batched step (LDE + leaf hashing + compression)", "bound": "int",
                      "unit": "Gmul/s", "achieved": ach, "peak": mul_peak / 1e9, "frac": ach / (mul_peak / 1e9),
                      "peak_source": "measured in this run: zkb_measure_mul_peak",
@@ -781,7 +819,6 @@ def run_batch(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
-    batch.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
