@@ -1,6 +1,7 @@
 // engine.cuh — internal host-side interfaces between the CUDA modules.
 #pragma once
 #include <chrono>
+#include <map>
 #include <array>
 #include <condition_variable>
 #include <memory>
@@ -136,15 +137,19 @@ struct FriProof {
 // uploads the one with the fewest bytes left goes next (ties: the earlier request): an
 // upload in progress keeps the link against a later one of equal size, so equal jobs upload
 // one after another and the first starts computing early, while a small job's upload waits
-// for at most one piece of a large one.
+// for at most one piece of a large one.  A waiting piece passed over `max_bypass` times
+// goes next, so a steady stream of smaller uploads cannot hold a large job's upload (and
+// the memory it was admitted with) back without bound.
 class UploadGate {
  public:
+  explicit UploadGate(uint32_t max_bypass = 8) : max_bypass_(max_bypass) {}
   void acquire(uint64_t bytes_left) {
     std::unique_lock<std::mutex> lk(mu_);
     const std::pair<uint64_t, uint64_t> key{bytes_left, next_++};
-    waiting_.insert(key);
-    cv_.wait(lk, [&] { return !busy_ && *waiting_.begin() == key; });
-    waiting_.erase(waiting_.begin());
+    waiting_[key] = 0;
+    cv_.wait(lk, [&] { return !busy_ && chosen() == key; });
+    waiting_.erase(key);
+    for (auto &w : waiting_) w.second++;  // every other waiter was passed over once more
     busy_ = true;
   }
   void release() {
@@ -156,11 +161,19 @@ class UploadGate {
   }
 
  private:
+  // the earliest request passed over max_bypass times, else the fewest bytes left
+  std::pair<uint64_t, uint64_t> chosen() const {
+    const std::pair<uint64_t, uint64_t> *pick = nullptr;
+    for (auto &w : waiting_)
+      if (w.second >= max_bypass_ && (!pick || w.first.second < pick->second)) pick = &w.first;
+    return pick ? *pick : waiting_.begin()->first;
+  }
   std::mutex mu_;
   std::condition_variable cv_;
-  std::set<std::pair<uint64_t, uint64_t>> waiting_;
+  std::map<std::pair<uint64_t, uint64_t>, uint32_t> waiting_;  // (bytes left, request) -> times passed over
   uint64_t next_ = 0;
   bool busy_ = false;
+  const uint32_t max_bypass_;
 };
 
 // One PCS commit job from host memory (+ FRI when `fri` is set), device state released.

@@ -115,7 +115,9 @@ struct zkb_engine {
   uint64_t budget = 0, in_use = 0;
   uint32_t policy = ZKB_ADMIT_FIFO;
   std::mutex mu;
-  UploadGate upload_mu;  // one trace piece crosses PCIe at a time, the fewest bytes left first
+  // one trace piece crosses PCIe at a time, the fewest bytes left first; a piece passed
+  // over ZKB_ADMIT_MAX_BYPASS times goes next
+  UploadGate upload_mu{ZKB_ADMIT_MAX_BYPASS};
   // One job of each size class runs its LDE and tree at a time: equal jobs pipeline one's
   // upload under another's kernels instead of interleaving their kernels block by block;
   // jobs of different classes still overlap, the smaller at the higher stream priority.
