@@ -142,7 +142,7 @@ struct FriProof {
 // the memory it was admitted with) back without bound.
 class UploadGate {
  public:
-  explicit UploadGate(uint32_t max_bypass = 8) : max_bypass_(max_bypass) {}
+  explicit UploadGate(uint32_t max_bypass = 64) : max_bypass_(max_bypass) {}
   void acquire(uint64_t bytes_left) {
     std::unique_lock<std::mutex> lk(mu_);
     const std::pair<uint64_t, uint64_t> key{bytes_left, next_++};

@@ -116,8 +116,9 @@ struct zkb_engine {
   uint32_t policy = ZKB_ADMIT_FIFO;
   std::mutex mu;
   // one trace piece crosses PCIe at a time, the fewest bytes left first; a piece passed
-  // over ZKB_ADMIT_MAX_BYPASS times goes next
-  UploadGate upload_mu{ZKB_ADMIT_MAX_BYPASS};
+  // over 64 times (16 GiB of other uploads) goes next — more than the 4.3 GB uploads of
+  // equal jobs submitted together, which keep uploading one after another
+  UploadGate upload_mu{64};
   // One job of each size class runs its LDE and tree at a time: equal jobs pipeline one's
   // upload under another's kernels instead of interleaving their kernels block by block;
   // jobs of different classes still overlap, the smaller at the higher stream priority.
