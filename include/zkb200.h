@@ -172,6 +172,17 @@ ZKB_API int zkb_dft_batch_dev(int field, void *d_rowmajor, uint32_t log_h, uint3
 ZKB_API int zkb_dft_batch_noalloc_dev(int field, void *d_rowmajor, uint32_t log_h, uint32_t width,
                                       int inverse, void *stream);
 
+/* Tile loads of the BabyBear NTT passes (DFT, LDE, commits; process-wide): 0 = coalesced
+ * loads straight into registers (the default); 1 = one tensor copy (TMA,
+ * cp.async.bulk.tensor, no multicast) of each pass tile into shared memory, used where the
+ * rows are 16-byte aligned (width a multiple of 4, column chunks of 4 or more; other passes
+ * keep the loads).  ZKB_NTT_TMA=1 in the environment selects 1 at load.  Results are the
+ * same bit for bit.  No counterpart in the reference. */
+ZKB_API int zkb_set_ntt_tile_loads(int mode);
+/* Tensor-copy waits of the NTT passes that gave up (bounded polls) since the last call;
+ * nonzero means those passes' outputs are invalid.  Resets the count. */
+ZKB_API int zkb_ntt_tile_load_errors(uint32_t *count);
+
 /* p3 coset_lde_batch(trace, log_blowup, shift) followed, when bitrev_rows=1, by
  * bit_reverse_rows — the LDE that TwoAdicFriPcs::commit hands to the MMCS
  * (zkf-backends/src/plonky3.rs:250-262 -> p3-dft 0.4.2;
@@ -537,6 +548,15 @@ ZKB_API int zkb_batch_trace_ptr(zkb_batch *batch, size_t i, void **d_trace);
 /* Copies trace i in from host (pinned for full bandwidth) or device memory. */
 ZKB_API int zkb_batch_copy_in(zkb_batch *batch, size_t i, const void *src, int src_on_device, void *stream);
 ZKB_API int zkb_batch_run(zkb_batch *batch, void *stream);
+/* One run whose traces come from host memory: traces[i] points to trace i (2^log_h x width,
+ * row-major, canonical elements; pinned host memory for the copies to run asynchronously).
+ * The copies overlap the commitment: one copy stream takes the traces smallest first, and
+ * each trace's LDE and its own tree start on its branch as soon as its copy has landed
+ * (per-trace tree launches instead of the graph's joint ones).  A persistent
+ * plan copies every trace first, then runs its kernel.  Pinned sources are read until
+ * `stream` has passed the run; pageable ones are staged before the call returns.  Roots
+ * and trees as after zkb_batch_run.  No counterpart in the reference. */
+ZKB_API int zkb_batch_run_host(zkb_batch *batch, const void *const *traces, void *stream);
 /* n x OUT root elements (Goldilocks digests as u64); synchronises `stream`. */
 ZKB_API int zkb_batch_roots(zkb_batch *batch, void *roots_out, void *stream);
 /* Borrowed tree of trace i (valid while the plan lives, contents after a finished run):

@@ -174,3 +174,102 @@ def test_config4_shape_distribution_at_reduced_height():
     want = _plain_roots(Z.BABYBEAR, traces)
     _, got = _batch_roots(Z.BABYBEAR, shapes, traces, autotune=True)
     assert all((g == w).all() for g, w in zip(got, want))
+
+
+# ---- runs from host memory (zkb_batch_run_host): copies overlapped with the commitment,
+# traces committed in groups (smallest first) as their copies land
+
+
+@pytest.mark.parametrize("branches,use_graph", [(1, True), (3, True), (2, False)])
+def test_run_host_roots_equal_plain_commits(branches, use_graph):
+    b = Z.BatchCommit(MIXED, autotune=False, branches=branches, use_graph=use_graph)
+    for rep in range(2):
+        traces = _traces(Z.BABYBEAR, MIXED, 1300 + 40 * rep)
+        b.run_host(traces)
+        got = b.roots()
+        want = _plain_roots(Z.BABYBEAR, traces)
+        for i in range(len(MIXED)):
+            assert (got[i] == want[i]).all(), f"rep {rep} trace {i} shape {MIXED[i]}"
+
+
+def test_run_host_pinned_sources_alternating_with_graph_runs():
+    import torch
+
+    shapes = MIXED[:7]
+    b = Z.BatchCommit(shapes, autotune=False)
+    for rep in range(3):
+        traces = _traces(Z.BABYBEAR, shapes, 1400 + 30 * rep)
+        want = _plain_roots(Z.BABYBEAR, traces)
+        pinned = [torch.from_numpy(t.view(np.int32)).pin_memory() for t in traces]
+        b.run_host(pinned)
+        got = b.roots()
+        assert all((g == w).all() for g, w in zip(got, want)), f"rep {rep} run_host"
+        # the graph form on the same plan after a host run, with other traces
+        other = _traces(Z.BABYBEAR, shapes, 1500 + 30 * rep)
+        for i, t in enumerate(other):
+            b.copy_in(i, t)
+        b.run()
+        got = b.roots()
+        want2 = _plain_roots(Z.BABYBEAR, other)
+        assert all((g == w).all() for g, w in zip(got, want2)), f"rep {rep} graph run"
+
+
+@pytest.mark.parametrize("p2w", [16, 12])
+def test_run_host_goldilocks(p2w):
+    shapes = [(1 << 10, 64), (1 << 7, 8), (1 << 12, 12), (1 << 3, 1)]
+    traces = _traces(Z.GOLDILOCKS, shapes, 1600)
+    want = _plain_roots(Z.GOLDILOCKS, traces, log_blowup=2, p2w=p2w)
+    b = Z.BatchCommit(shapes, field=Z.GOLDILOCKS, log_blowup=2, p2_width=p2w, autotune=False, branches=2)
+    b.run_host(traces)
+    assert all((g == w).all() for g, w in zip(b.roots(), want))
+
+
+def test_run_host_persistent_plan():
+    shapes = [(1 << 12, 16), (1 << 9, 8), (1 << 14, 24), (1 << 6, 64)]
+    traces = _traces(Z.BABYBEAR, shapes, 1700)
+    want = _plain_roots(Z.BABYBEAR, traces)
+    b = Z.BatchCommit(shapes, persistent=True, autotune=False)
+    b.run_host(traces)
+    assert all((g == w).all() for g, w in zip(b.roots(), want))
+
+
+def test_openings_after_run_host():
+    traces = _traces(Z.BABYBEAR, MIXED, 1800)
+    b = Z.BatchCommit(MIXED, autotune=False, branches=2)
+    b.run_host(traces)
+    b.roots()
+    pcs = Z.CudaTwoAdicPcs(Z.BABYBEAR, 42, 1)
+    for i in (2, 6, 9):
+        _, plain_tree = pcs.commit(traces[i])
+        n = MIXED[i][0] << 1
+        for idx in (0, n - 1, n // 5):
+            got = pcs.mmcs.open_batch(idx, b.tree(i))
+            want = pcs.mmcs.open_batch(idx, plain_tree)
+            assert all((x == y).all() for x, y in zip(got[0], want[0]))
+            assert all((x == y).all() for x, y in zip(got[1], want[1]))
+
+
+def test_run_host_rejects_bad_sources():
+    import torch
+
+    shapes = [(1 << 4, 8), (1 << 5, 3)]
+    b = Z.BatchCommit(shapes, autotune=False)
+    traces = _traces(Z.BABYBEAR, shapes, 1900)
+    with pytest.raises(ValueError):
+        b.run_host(traces[:1])
+    with pytest.raises(ValueError):
+        b.run_host([traces[1], traces[0]])
+    with pytest.raises(ValueError):
+        b.run_host([torch.from_numpy(traces[0].view(np.int32)).cuda(), traces[1]])
+
+
+def test_run_host_many_groups():
+    # 40 traces of growing size: the smallest share groups, the largest stand alone
+    shapes = [(1 << (4 + i % 9), 8 + 8 * (i % 5)) for i in range(40)]
+    traces = _traces(Z.BABYBEAR, shapes, 2000)
+    want = _plain_roots(Z.BABYBEAR, traces)
+    b = Z.BatchCommit(shapes, autotune=False, branches=4)
+    b.run_host(traces)
+    got = b.roots()
+    for i in range(len(shapes)):
+        assert (got[i] == want[i]).all(), f"trace {i} shape {shapes[i]}"

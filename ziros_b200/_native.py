@@ -134,6 +134,8 @@ SIGNATURES = {
     "zkb_dft_batch": (_I, [_I, _P, _U32, _U32, _I]),
     "zkb_dft_batch_dev": (_I, [_I, _P, _U32, _U32, _I, _P]),
     "zkb_dft_batch_noalloc_dev": (_I, [_I, _P, _U32, _U32, _I, _P]),
+    "zkb_set_ntt_tile_loads": (_I, [_I]),
+    "zkb_ntt_tile_load_errors": (_I, [_P]),
     "zkb_coset_lde_batch": (_I, [_I, _P, _U32, _U32, _U32, _U64, _I, _P]),
     "zkb_coset_lde_batch_dev": (_I, [_I, _P, _U32, _U32, _U32, _U64, _I, _P, _P]),
     "zkb_mmcs_commit": (_I, [_P, _P, _SZ, _P, _P]),
@@ -204,6 +206,7 @@ SIGNATURES = {
     "zkb_batch_trace_ptr": (_I, [_P, _SZ, _P]),
     "zkb_batch_copy_in": (_I, [_P, _SZ, _P, _I, _P]),
     "zkb_batch_run": (_I, [_P, _P]),
+    "zkb_batch_run_host": (_I, [_P, _P, _P]),
     "zkb_batch_roots": (_I, [_P, _P, _P]),
     "zkb_batch_tree": (_I, [_P, _SZ, _P]),
     "zkb_batch_info": (_I, [_P, _P]),
@@ -270,6 +273,18 @@ def device_allocations() -> int:
 def release_cached_memory() -> None:
     """Returns the library's cached device blocks and the pool's unused memory to the device."""
     check(load().zkb_release_cached_memory())
+
+
+def set_ntt_tile_loads(mode: int) -> None:
+    """BabyBear NTT pass tiles: 0 = loads into registers (default), 1 = one tensor copy per tile."""
+    check(load().zkb_set_ntt_tile_loads(int(mode)))
+
+
+def ntt_tile_load_errors() -> int:
+    """Tensor-copy waits of the NTT passes that gave up since the last call (resets)."""
+    n = C.c_uint32(0)
+    check(load().zkb_ntt_tile_load_errors(C.byref(n)))
+    return n.value
 
 
 def last_error() -> str:

@@ -840,6 +840,30 @@ class BatchCommit:
     def run(self, stream=None) -> None:
         N.check(N.load().zkb_batch_run(self._h, stream))
 
+    def run_host(self, traces, stream=None) -> None:
+        """One run from host memory, the copies overlapped with the commitment
+        (zkb_batch_run_host).  traces: one per shape, host arrays (staged before the call
+        returns) or pinned host torch tensors (asynchronous: keep them alive until the
+        stream has passed the run)."""
+        if len(traces) != len(self.shapes):
+            raise ValueError("one trace per shape")
+        isz = np.dtype(dtype_of(self.field)).itemsize
+        keep, ptrs = [], (C.c_void_p * len(self.shapes))()
+        for i, (t, (h, w)) in enumerate(zip(traces, self.shapes)):
+            if hasattr(t, "is_cuda"):
+                if t.is_cuda or tuple(t.shape) != (h, w) or t.element_size() != isz or not t.is_contiguous():
+                    raise ValueError(f"trace {i}: a contiguous host tensor of shape {(h, w)} expected")
+                if stream is None:
+                    stream = _current_stream(None)
+                ptrs[i] = t.data_ptr()
+            else:
+                a = np.ascontiguousarray(t, dtype=dtype_of(self.field))
+                if a.shape != (h, w):
+                    raise ValueError(f"trace {i}: shape {a.shape}, expected {(h, w)}")
+                keep.append(a)
+                ptrs[i] = a.ctypes.data
+        N.check(N.load().zkb_batch_run_host(self._h, ptrs, stream))
+
     def set_merkle_fusion(self, leaf_levels: int, comp_levels: int) -> None:
         """Persistent plans: Merkle levels the leaf tile computes above the leaves (0..8)
         and levels per compression tile (1..8)."""
@@ -898,6 +922,9 @@ class BatchCommit:
 
 
 def _current_stream(t):
+    """torch's current stream on the tensor's device (the current device for host tensors)."""
     import torch
 
+    if t is None or not t.is_cuda:
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
     return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)

@@ -263,6 +263,19 @@ int zkb_dft_batch_dev(int field, void *d, uint32_t log_h, uint32_t width, int in
   return ntt_dft_dev<Goldilocks>((uint64_t *)d, (int)log_h, width, inverse != 0, s);
 }
 
+int zkb_set_ntt_tile_loads(int mode) {
+  clear_error();
+  ZKB_REQUIRE(mode == 0 || mode == 1, "tile load mode %d (0: loads into registers, 1: tensor copies)", mode);
+  set_ntt_tile_loads(mode);
+  return ZKB_OK;
+}
+
+int zkb_ntt_tile_load_errors(uint32_t *count) {
+  ZKB_ENTRY();
+  ZKB_REQUIRE(count != nullptr, "null count");
+  return ntt_tma_wait_errors(count);
+}
+
 int zkb_dft_batch(int field, void *rowmajor, uint32_t log_h, uint32_t width, int inverse) {
   ZKB_ENTRY();
   ZKB_TRY(check_field(field));
@@ -414,9 +427,10 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
       // link is taken per 256 MiB piece, the upload with the fewest bytes left first, so a
       // small job's upload waits for one piece of a large job's, not for all of it.
       const size_t total = n * width * es, piece = 256ull << 20;
+      const uint64_t ticket = upload_mu->ticket();
       for (size_t off = 0; off < total; off += piece) {
         const size_t len = total - off < piece ? total - off : piece;
-        upload_mu->acquire(total - off);
+        upload_mu->acquire(total - off, ticket);
         int rc = ZKB_OK;
         const cudaError_t e = cudaMemcpyAsync((char *)staged.p + off, (const char *)h_trace + off, len,
                                               cudaMemcpyHostToDevice, s);

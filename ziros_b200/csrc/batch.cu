@@ -48,6 +48,28 @@ constexpr int MAX_BATCH = 1024;
 using mt::CompJob;
 using mt::LeafJob;
 
+// Job tables of a set of trees: host copy and device pointers (root_dst: the batch index
+// of each root, NULL when the set is the whole batch in order).
+struct JobTables {
+  mt::Tables t;
+  const LeafJob *leaf = nullptr;
+  const CompJob *comp = nullptr;
+  const uint64_t *root_off = nullptr;
+  const uint32_t *root_dst = nullptr;
+};
+
+// A group of a run from host memory: traces consecutive in the copy order (smallest
+// first), committed together once their copies have landed — their LDEs over the
+// branches, then one multi-tree launch set — as one graph (or the same launches).
+struct HostGroup {
+  std::vector<int> traces;
+  std::vector<char> member;  // per batch index
+  JobTables jobs;
+  cudaEvent_t copied = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
 uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
 
 uint64_t fnv1a(const void *data, size_t n, uint64_t h = 1469598103934665603ull) {
@@ -124,10 +146,7 @@ struct zkb_batch {
   std::vector<void *> d_coef;                    // per branch: scratch for its largest trace
   uint64_t coef_bytes = 0;
   void *d_roots = nullptr;
-  uint64_t *d_root_off = nullptr;  // digest offsets of the roots from d_layers[0]
-  LeafJob *d_leaf_jobs = nullptr;
-  CompJob *d_comp_jobs = nullptr;
-  mt::Tables tables;
+  JobTables joint;  // every trace's tree, roots in batch order
   // kernel shapes
   std::vector<LdeTune> tune;  // per trace
   unsigned leaf_threads = 128;
@@ -151,6 +170,10 @@ struct zkb_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint32_t kernels_per_run = 0;
+  // runs from host memory (run_host): copy stream and the groups of the copy order
+  cudaStream_t s_copy = nullptr;
+  cudaEvent_t ev_host = nullptr, ev_copied = nullptr;
+  std::vector<HostGroup> host_groups;
   P2Params<BabyBear, 16> p_bb16;
   P2Params<Goldilocks, 16> p_gl16;
   P2Params<Goldilocks, 12> p_gl12;
@@ -166,7 +189,15 @@ struct zkb_batch {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     for (auto e : ev_br) cudaEventDestroy(e);
+    for (auto &g : host_groups) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      if (g.graph) cudaGraphDestroy(g.graph);
+      if (g.copied) cudaEventDestroy(g.copied);
+    }
+    if (ev_host) cudaEventDestroy(ev_host);
+    if (ev_copied) cudaEventDestroy(ev_copied);
     if (ev_fork) cudaEventDestroy(ev_fork);
+    if (s_copy) cudaStreamDestroy(s_copy);
     for (auto s : s_br) cudaStreamDestroy(s);
     if (s_main) cudaStreamDestroy(s_main);
     if (arena) cudaFree(arena);
@@ -192,16 +223,118 @@ struct zkb_batch {
     return 0;
   }
 
+  // The trees of a set of traces: one leaf-hash launch over all their rows, one
+  // compression launch per level, one root gather.
   template <class F, int W>
-  int hash_all(const P2Params<F, W> &p, unsigned threads, cudaStream_t s) {
-    return mt::launch_trees<F, W>(tables, d_leaf_jobs, d_comp_jobs, d_root_off, d_layers[0], d_roots, p, threads, s,
-                                  "batch_leaf_hash", "batch_compress", "batch_roots");
+  int hash_set(const JobTables &j, const P2Params<F, W> &p, unsigned threads, cudaStream_t s) {
+    return mt::launch_trees<F, W>(j.t, j.leaf, j.comp, j.root_off, d_layers[0], d_roots, p, threads, s,
+                                  "batch_leaf_hash", "batch_compress", "batch_roots", j.root_dst);
   }
 
-  int hash_dispatch(unsigned threads, cudaStream_t s) {
-    if (spec.field == FIELD_BABYBEAR) return hash_all<BabyBear, 16>(p_bb16, threads, s);
-    if (spec.width == 16) return hash_all<Goldilocks, 16>(p_gl16, threads, s);
-    return hash_all<Goldilocks, 12>(p_gl12, threads, s);
+  int hash_tables(const JobTables &j, unsigned threads, cudaStream_t s) {
+    if (spec.field == FIELD_BABYBEAR) return hash_set<BabyBear, 16>(j, p_bb16, threads, s);
+    if (spec.width == 16) return hash_set<Goldilocks, 16>(j, p_gl16, threads, s);
+    return hash_set<Goldilocks, 12>(j, p_gl12, threads, s);
+  }
+
+  int hash_dispatch(unsigned threads, cudaStream_t s) { return hash_tables(joint, threads, s); }
+
+  // The LDEs of the `member` traces (every trace when NULL), forked over their branches
+  // (each branch in its own order, with its own coefficient scratch) and joined on origin.
+  int enqueue_ldes(const std::vector<char> *member, cudaStream_t origin) {
+    const uint32_t nb = (uint32_t)branch_traces.size();
+    ZKB_CHECK_CUDA(cudaEventRecord(ev_fork, origin));
+    for (uint32_t b = 0; b < nb; b++) {
+      bool any = !member;
+      for (int i : branch_traces[b]) any = any || (*member)[i];
+      if (!any) continue;
+      ZKB_CHECK_CUDA(cudaStreamWaitEvent(s_br[b], ev_fork, 0));
+      for (int i : branch_traces[b])
+        if (!member || (*member)[i]) ZKB_TRY(lde_one((size_t)i, s_br[b], &tune[i]));
+      ZKB_CHECK_CUDA(cudaEventRecord(ev_br[b], s_br[b]));
+      ZKB_CHECK_CUDA(cudaStreamWaitEvent(origin, ev_br[b], 0));
+    }
+    return ZKB_OK;
+  }
+
+  int enqueue_group(const HostGroup &g, cudaStream_t origin) {
+    ZKB_TRY(enqueue_ldes(&g.member, origin));
+    return hash_tables(g.jobs, leaf_threads, origin);
+  }
+
+  // One graph per host group (the group's launches captured on s_main).
+  int capture_groups() {
+    for (auto &g : host_groups) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      if (g.graph) cudaGraphDestroy(g.graph);
+      g.exec = nullptr;
+      g.graph = nullptr;
+      ZKB_CHECK_CUDA(cudaStreamBeginCapture(s_main, cudaStreamCaptureModeRelaxed));
+      const int rc = enqueue_group(g, s_main);
+      cudaGraph_t gr = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(s_main, &gr);
+      ZKB_TRY(rc);
+      if (e != cudaSuccess) {
+        set_error("graph capture failed: %s", cudaGetErrorString(e));
+        return ZKB_ERR_CUDA;
+      }
+      g.graph = gr;
+      ZKB_CHECK_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    }
+    return ZKB_OK;
+  }
+
+  int copy_host(size_t i, const void *src, cudaStream_t s) {
+    const uint64_t bytes = (1ull << shapes[i].log_h) * shapes[i].width * es;
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(d_in[i], src, bytes, cudaMemcpyHostToDevice, s));
+    return ZKB_OK;
+  }
+
+  // A run whose traces come from host memory, the copies overlapped with the commitment:
+  // the copy stream takes the traces smallest first, in groups (consecutive in that order,
+  // growing from about 1/64 of the batch's cells to at most 1/16; a larger trace is a group
+  // by itself), and each group's LDEs and trees run on origin as soon as its last copy has
+  // landed, while the next groups copy.  A trace's commitment takes longer than its copy at
+  // any size (the rates are near proportional), so smallest first is Johnson's order for a
+  // two-stage flow (copy, then compute): compute starts after the first, small group's copy
+  // and is not left waiting after that, and the last group, whose compute follows the last
+  // copy, is at most one large trace or 1/16 of the batch.  Copies and launches are
+  // enqueued group by group, so a pageable source (staged by the copy call) still overlaps
+  // the staging of later groups with the work on earlier ones.  A persistent plan reads
+  // every trace from its one kernel: its copies all go first.
+  int run_host(const void *const *src, cudaStream_t origin) {
+    const size_t n = shapes.size();
+    for (size_t i = 0; i < n; i++) ZKB_REQUIRE(src[i] != nullptr, "trace %zu: null host source", i);
+    ZKB_CHECK_CUDA(cudaEventRecord(ev_host, origin));
+    ZKB_CHECK_CUDA(cudaStreamWaitEvent(s_copy, ev_host, 0));
+    int rc = ZKB_OK;
+    if (persistent) {
+      for (size_t i = 0; i < n && rc == ZKB_OK; i++) rc = copy_host(i, src[i], s_copy);
+    } else {
+      for (size_t k = 0; k < host_groups.size() && rc == ZKB_OK; k++) {
+        HostGroup &g = host_groups[k];
+        for (size_t q = 0; q < g.traces.size() && rc == ZKB_OK; q++) rc = copy_host(g.traces[q], src[g.traces[q]], s_copy);
+        if (rc != ZKB_OK) break;
+        if (cudaEventRecord(g.copied, s_copy) != cudaSuccess || cudaStreamWaitEvent(origin, g.copied, 0) != cudaSuccess) {
+          set_error("copy ordering failed: %s", cudaGetErrorString(cudaGetLastError()));
+          rc = ZKB_ERR_CUDA;
+          break;
+        }
+        if (g.exec) {
+          if (cudaGraphLaunch(g.exec, origin) != cudaSuccess) {
+            set_error("group graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            rc = ZKB_ERR_CUDA;
+          }
+        } else {
+          rc = enqueue_group(g, origin);
+        }
+      }
+    }
+    // origin joins the copy stream, also after an error (the sources are read until then)
+    ZKB_CHECK_CUDA(cudaEventRecord(ev_copied, s_copy));
+    ZKB_CHECK_CUDA(cudaStreamWaitEvent(origin, ev_copied, 0));
+    ZKB_TRY(rc);
+    return persistent ? persist->enqueue(origin) : ZKB_OK;
   }
 
   // The persistent form's plan over the current kernel shapes and Merkle fusion.
@@ -233,14 +366,7 @@ struct zkb_batch {
 
   int enqueue(cudaStream_t origin) {
     if (persistent) return persist->enqueue(origin);
-    const uint32_t nb = (uint32_t)branch_traces.size();
-    ZKB_CHECK_CUDA(cudaEventRecord(ev_fork, origin));
-    for (uint32_t b = 0; b < nb; b++) {
-      ZKB_CHECK_CUDA(cudaStreamWaitEvent(s_br[b], ev_fork, 0));
-      for (int i : branch_traces[b]) ZKB_TRY(lde_one((size_t)i, s_br[b], &tune[i]));
-      ZKB_CHECK_CUDA(cudaEventRecord(ev_br[b], s_br[b]));
-      ZKB_CHECK_CUDA(cudaStreamWaitEvent(origin, ev_br[b], 0));
-    }
+    ZKB_TRY(enqueue_ldes(nullptr, origin));
     return hash_dispatch(leaf_threads, origin);
   }
 
@@ -583,6 +709,11 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   for (size_t i = 0; i < n; i++) n_comp += b->shapes[i].log_h + b->log_b;
   const uint64_t tables_off = off;
   off = align256(off + n * sizeof(LeafJob) + n_comp * sizeof(CompJob) + n * 8);
+  // the same jobs once more as one table set per host group (runs from host memory): the
+  // jobs, root offsets and root indices of each group, every group's records 8-byte aligned
+  const uint64_t group_tables_off = off;
+  const uint64_t group_tables_bytes = n * (sizeof(LeafJob) + 8 + 4 + 8) + n_comp * sizeof(CompJob);
+  off = align256(off + group_tables_bytes);
   b->arena_bytes = off;
 
   size_t free_b = 0, total_b = 0;
@@ -652,12 +783,86 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
     rows[i] = b->rows_of(i);
     widths[i] = b->shapes[i].width;
   }
-  mt::build_tables(data, rows, widths, b->d_layers, b->d_layers[0], OUT, es, &b->tables);
-  ZKB_REQUIRE(b->tables.device_bytes() <= n * sizeof(LeafJob) + n_comp * sizeof(CompJob) + n * 8,
+  mt::build_tables(data, rows, widths, b->d_layers, b->d_layers[0], OUT, es, &b->joint.t);
+  ZKB_REQUIRE(b->joint.t.device_bytes() <= n * sizeof(LeafJob) + n_comp * sizeof(CompJob) + n * 8,
               "internal: batch job tables");
   ZKB_CHECK_CUDA(cudaMemsetAsync(b->arena, 0, layers_base, b->s_main));
-  ZKB_TRY(mt::upload_tables(b->tables, base + tables_off, b->s_main, &b->d_leaf_jobs, &b->d_comp_jobs,
-                            &b->d_root_off));
+  {
+    LeafJob *l = nullptr;
+    CompJob *c = nullptr;
+    uint64_t *r = nullptr;
+    ZKB_TRY(mt::upload_tables(b->joint.t, base + tables_off, b->s_main, &l, &c, &r));
+    b->joint.leaf = l;
+    b->joint.comp = c;
+    b->joint.root_off = r;
+  }
+  // host groups: traces by cells, fewest first; a group closes once it holds `target`
+  // cells (about 1/64 of the batch, doubling per group up to 1/16) or before a trace
+  // that would take it past that; a larger trace forms a group by itself
+  std::vector<char> img;
+  if (!b->persistent) {
+    auto cells = [&](int i) { return (uint64_t)b->shapes[i].width << b->shapes[i].log_h; };
+    std::vector<int> ord(n);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cells(x) < cells(y); });
+    uint64_t total = 0;
+    for (size_t i = 0; i < n; i++) total += cells((int)i);
+    const uint64_t cap = std::max<uint64_t>(total / 16, 1);
+    uint64_t target = std::min<uint64_t>(cap, std::max<uint64_t>(total / 64, 1ull << 20)), acc = 0;
+    std::vector<std::vector<int>> groups(1);
+    for (int i : ord) {
+      if (!groups.back().empty() && acc + cells(i) > target) {
+        groups.emplace_back();
+        acc = 0;
+        target = std::min(cap, 2 * target);
+      }
+      groups.back().push_back(i);
+      acc += cells(i);
+      if (acc >= target) {
+        groups.emplace_back();
+        acc = 0;
+        target = std::min(cap, 2 * target);
+      }
+    }
+    if (groups.back().empty()) groups.pop_back();
+    img.assign(group_tables_bytes, 0);
+    uint64_t to = 0;
+    b->host_groups.resize(groups.size());
+    for (size_t k = 0; k < groups.size(); k++) {
+      HostGroup &g = b->host_groups[k];
+      g.traces = groups[k];
+      g.member.assign(n, 0);
+      const size_t m = g.traces.size();
+      std::vector<const void *> gd(m);
+      std::vector<uint64_t> gr(m), gw(m);
+      std::vector<void *> gl(m);
+      std::vector<uint32_t> dst(m);
+      for (size_t q = 0; q < m; q++) {
+        const int i = g.traces[q];
+        g.member[i] = 1;
+        gd[q] = data[i];
+        gr[q] = rows[i];
+        gw[q] = widths[i];
+        gl[q] = b->d_layers[i];
+        dst[q] = (uint32_t)i;
+      }
+      mt::build_tables(gd, gr, gw, gl, b->d_layers[0], OUT, es, &g.jobs.t);
+      const uint64_t lb = m * sizeof(LeafJob), cb = g.jobs.t.comp.size() * sizeof(CompJob), rb = m * 8,
+                     db = (m * 4 + 7) & ~7ull;
+      ZKB_REQUIRE(to + lb + cb + rb + db <= group_tables_bytes, "internal: host group job tables");
+      char *dev = base + group_tables_off + to;
+      memcpy(img.data() + to, g.jobs.t.leaf.data(), lb);
+      if (cb) memcpy(img.data() + to + lb, g.jobs.t.comp.data(), cb);
+      memcpy(img.data() + to + lb + cb, g.jobs.t.root_off.data(), rb);
+      memcpy(img.data() + to + lb + cb + rb, dst.data(), m * 4);
+      g.jobs.leaf = (const LeafJob *)dev;
+      g.jobs.comp = (const CompJob *)(dev + lb);
+      g.jobs.root_off = (const uint64_t *)(dev + lb + cb);
+      g.jobs.root_dst = (const uint32_t *)(dev + lb + cb + rb);
+      to += lb + cb + rb + db;
+    }
+    ZKB_CHECK_CUDA(cudaMemcpyAsync(base + group_tables_off, img.data(), to, cudaMemcpyHostToDevice, b->s_main));
+  }
   ZKB_TRY(wait_stream(b->s_main));
 
   // ---- streams and events
@@ -670,6 +875,10 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
     b->ev_br.push_back(e);
   }
   ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  ZKB_CHECK_CUDA(cudaStreamCreateWithFlags(&b->s_copy, cudaStreamNonBlocking));
+  ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&b->ev_host, cudaEventDisableTiming));
+  ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&b->ev_copied, cudaEventDisableTiming));
+  for (auto &g : b->host_groups) ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&g.copied, cudaEventDisableTiming));
 
   // ---- tables (built once, outside any capture) and kernel shapes
   b->tune.assign(n, LdeTune{});
@@ -701,6 +910,7 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   ZKB_TRY(rc);
   if (opt.autotune) cache.save();
   if (b->use_graph) ZKB_TRY(b->capture());
+  if (b->use_graph && !b->persistent) ZKB_TRY(b->capture_groups());
 
   // ---- borrowed per-trace trees for openings
   for (size_t i = 0; i < n; i++) {
@@ -712,7 +922,7 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
     d.d_layers = b->d_layers[i];
     d.borrowed = true;
     uint64_t o = 0;
-    for (uint64_t len : b->tables.layer_len[i]) {
+    for (uint64_t len : b->joint.t.layer_len[i]) {
       d.layer_off.push_back(o);
       d.layer_len.push_back(len);
       o += len;
@@ -803,6 +1013,14 @@ int zkb_batch_run(zkb_batch *b, void *stream) {
   ZKB_TRY(library_gate());
   ZKB_CHECK_CUDA(cudaSetDevice(b->device));
   return b->run(resolve_stream(stream));
+}
+
+int zkb_batch_run_host(zkb_batch *b, const void *const *traces, void *stream) {
+  clear_error();
+  ZKB_REQUIRE(b && traces, "null arguments");
+  ZKB_TRY(library_gate());
+  ZKB_CHECK_CUDA(cudaSetDevice(b->device));
+  return b->run_host(traces, resolve_stream(stream));
 }
 
 int zkb_batch_roots(zkb_batch *b, void *roots_out, void *stream) {

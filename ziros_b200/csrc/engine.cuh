@@ -133,23 +133,35 @@ struct FriProof {
   ~FriProof();
 };
 
+// Tile loads of the BabyBear NTT passes (0 = coalesced loads into registers, 1 = one
+// tensor copy per tile), and the count of tensor-copy waits that gave up (reset on read).
+void set_ntt_tile_loads(int mode);
+int ntt_tile_loads_mode();
+int ntt_tma_wait_errors(uint32_t *count);
+
 // The PCIe link of an engine, handed out one trace piece at a time.  Among the waiting
-// uploads the one with the fewest bytes left goes next (ties: the earlier request): an
-// upload in progress keeps the link against a later one of equal size, so equal jobs upload
-// one after another and the first starts computing early, while a small job's upload waits
-// for at most one piece of a large one.  A waiting piece passed over `max_bypass` times
-// goes next, so a steady stream of smaller uploads cannot hold a large job's upload (and
-// the memory it was admitted with) back without bound.
+// uploads the one with the fewest bytes left goes next (ties: the earlier ticket, taken
+// once per upload): an upload in progress keeps the link against a later one of equal size,
+// so equal jobs upload one after another and the first starts computing early, while a
+// small job's upload waits for at most one piece of a large one.  A waiting upload that
+// pieces of later uploads have passed over `max_bypass` times goes next, so a steady stream
+// of smaller uploads cannot hold a large job's upload (and the memory it was admitted with)
+// back without bound; pieces of earlier uploads (the one in progress) do not count.
 class UploadGate {
  public:
   explicit UploadGate(uint32_t max_bypass = 64) : max_bypass_(max_bypass) {}
-  void acquire(uint64_t bytes_left) {
+  uint64_t ticket() {
+    std::lock_guard<std::mutex> lk(mu_);
+    return next_++;
+  }
+  void acquire(uint64_t bytes_left, uint64_t ticket) {
     std::unique_lock<std::mutex> lk(mu_);
-    const std::pair<uint64_t, uint64_t> key{bytes_left, next_++};
+    const std::pair<uint64_t, uint64_t> key{bytes_left, ticket};
     waiting_[key] = 0;
     cv_.wait(lk, [&] { return !busy_ && chosen() == key; });
     waiting_.erase(key);
-    for (auto &w : waiting_) w.second++;  // every other waiter was passed over once more
+    for (auto &w : waiting_)
+      if (w.first.second < ticket) w.second++;  // an earlier upload was passed over
     busy_ = true;
   }
   void release() {
@@ -161,7 +173,7 @@ class UploadGate {
   }
 
  private:
-  // the earliest request passed over max_bypass times, else the fewest bytes left
+  // the earliest upload passed over max_bypass times, else the fewest bytes left
   std::pair<uint64_t, uint64_t> chosen() const {
     const std::pair<uint64_t, uint64_t> *pick = nullptr;
     for (auto &w : waiting_)
@@ -170,7 +182,7 @@ class UploadGate {
   }
   std::mutex mu_;
   std::condition_variable cv_;
-  std::map<std::pair<uint64_t, uint64_t>, uint32_t> waiting_;  // (bytes left, request) -> times passed over
+  std::map<std::pair<uint64_t, uint64_t>, uint32_t> waiting_;  // (bytes left, ticket) -> times passed over
   uint64_t next_ = 0;
   bool busy_ = false;
   const uint32_t max_bypass_;

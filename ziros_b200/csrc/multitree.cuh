@@ -112,12 +112,16 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// roots[j] = the last digest of job j's layers (offsets in digests from `base`)
+// roots[dst[j]] = the last digest of job j's layers (offsets in digests from `base`;
+// dst NULL: roots[j])
 template <class T, int OUT>
 __global__ void mt_roots_kernel(const uint64_t *__restrict__ root_off, const T *__restrict__ base, int n,
-                                T *__restrict__ roots) {
+                                const uint32_t *__restrict__ dst, T *__restrict__ roots) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n * OUT) roots[t] = base[root_off[t / OUT] * OUT + (t % OUT)];
+  if (t < n * OUT) {
+    const int j = t / OUT;
+    roots[(uint64_t)(dst ? dst[j] : j) * OUT + (t % OUT)] = base[root_off[j] * OUT + (t % OUT)];
+  }
 }
 
 // Host-side job tables of a set of trees.  layers[j] points at job j's digest layers
@@ -200,7 +204,8 @@ inline int upload_tables(const Tables &t, void *dev, cudaStream_t s, LeafJob **d
 template <class F, int W>
 int launch_trees(const Tables &t, const LeafJob *d_leaf, const CompJob *d_comp, const uint64_t *d_root_off,
                  const void *base, void *d_roots, const P2Params<F, W> &p, unsigned leaf_threads,
-                 cudaStream_t s, const char *leaf_name, const char *comp_name, const char *root_name) {
+                 cudaStream_t s, const char *leaf_name, const char *comp_name, const char *root_name,
+                 const uint32_t *d_root_dst = nullptr) {
   using T = typename F::T;
   constexpr int OUT = digest_len<W>();
   DeviceContext *ctx;
@@ -214,7 +219,7 @@ int launch_trees(const Tables &t, const LeafJob *d_leaf, const CompJob *d_comp, 
   for (size_t l = 0; l < t.lvl_cnt.size(); l++) {
     ZKB_LAUNCH(comp_name, s, mt_compress_kernel<F, W><<<grid_for(t.lvl_total[l], 128, 1u << 30), 128, t.lvl_cnt[l] * sizeof(uint64_t), s>>>(d_comp + t.lvl_off[l], (int)t.lvl_cnt[l], t.lvl_total[l], p));
   }
-  ZKB_LAUNCH(root_name, s, mt_roots_kernel<T, OUT><<<(n * OUT + 127) / 128, 128, 0, s>>>(d_root_off, (const T *)base, n, (T *)d_roots));
+  ZKB_LAUNCH(root_name, s, mt_roots_kernel<T, OUT><<<(n * OUT + 127) / 128, 128, 0, s>>>(d_root_off, (const T *)base, n, d_root_dst, (T *)d_roots));
   return ZKB_OK;
 }
 

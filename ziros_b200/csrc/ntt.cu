@@ -21,6 +21,8 @@
 //
 // i.e. b independent size-n NR transforms of the coefficients twisted per coset.
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <type_traits>
 #include <utility>
 
@@ -262,6 +264,99 @@ __global__ void __launch_bounds__(C << LR2)
   ntt_pass_tile<F, LR1, LR2, C, false>(in, out, g, tw, post_scale, st, blockIdx.x, smem_raw);
 }
 
+// The same pass with its tile brought in by one tensor copy (BabyBear; see ntt_tile.cuh).
+// Thread 0 sets up the barrier and issues the copy, which runs while the block stages its
+// twiddles.
+template <int LR1, int LR2, int C>
+constexpr size_t tma_bar_off() {
+  return (pass_tile_smem<BabyBear, LR1, LR2, C>() + 15) & ~(size_t)15;
+}
+
+__device__ uint32_t g_tma_wait_errors;
+
+template <int LR1, int LR2, int C>
+__global__ void __launch_bounds__(C << LR2)
+    ntt_pass_tma_kernel(const uint32_t *in, uint32_t *out, const PassGeom g, const uint32_t *__restrict__ tw,
+                        uint32_t post_scale, const __grid_constant__ SmallTw<BabyBear> st,
+                        const __grid_constant__ CUtensorMap map) {
+  extern __shared__ __align__(128) unsigned char tma_smem[];  // the tensor copy's destination
+  constexpr int K = LR1 + LR2;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tma_smem + tma_bar_off<LR1, LR2, C>());
+  if (threadIdx.x == 0) {
+    const uint32_t chunk = blockIdx.x % g.chunks_per_row, rest = blockIdx.x / g.chunks_per_row;
+    const uint32_t grp = rest % g.groups, blk = rest / g.groups;
+    const uint32_t i_low = grp & ((1u << g.lo) - 1u);
+    const uint32_t high = blk * (g.groups >> g.lo) + (grp >> g.lo);  // row bits above the pass, transform
+    mbar_init(bar, 1);
+    mbar_expect_tx(bar, (uint32_t)(C << K) * 4u);
+    tma_load_5d(tma_smem, &map, bar, (int)(chunk * C), (int)i_low, 0, 0, (int)high);
+  }
+  __syncthreads();  // the barrier is initialised before anyone waits on it
+  ntt_pass_tile<BabyBear, LR1, LR2, C, false, true>(in, out, g, tw, post_scale, st, blockIdx.x, tma_smem, bar,
+                                                    &g_tma_wait_errors);
+}
+
+// Tile loads of the BabyBear passes: 0 = coalesced loads into registers (the default),
+// 1 = one tensor copy per tile.  Set by zkb_set_ntt_tile_loads or ZKB_NTT_TMA=1.
+std::atomic<int> &ntt_tile_loads() {
+  static std::atomic<int> mode{[] {
+    const char *v = getenv("ZKB_NTT_TMA");
+    return v && *v == '1' ? 1 : 0;
+  }()};
+  return mode;
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return (EncodeTiledFn)p;
+  }();
+  return fn;
+}
+
+// Tensor map of one column segment (`cols` columns from `base`, row stride g.width) for the
+// tiles of a K-bit pass at bits [g.lo, g.lo + K): dimensions (column, row bits below the
+// pass, the pass's bits split 8 + rest, the bits above with the transform index), box C
+// columns x 2^K rows.  The caller has checked: 4-byte elements, width % 4 == 0, base
+// 16-byte aligned, C >= 4 (every copy starts at a column that is a multiple of C).
+static int pass_tensor_map(CUtensorMap *m, const uint32_t *base, const PassGeom &g, uint32_t cols, int K,
+                           uint64_t n_blocks, uint32_t C) {
+  const EncodeTiledFn fn = encode_tiled();
+  ZKB_REQUIRE(fn != nullptr, "cuTensorMapEncodeTiled is not available");
+  const int K1 = K < 8 ? K : 8, K2 = K - K1;
+  const uint64_t row = (uint64_t)g.width * 4;
+  const cuuint64_t dims[5] = {cols, 1ull << g.lo, 1ull << K1, 1ull << K2, (1ull << (g.L - g.lo - K)) * n_blocks};
+  const cuuint64_t strides[4] = {row, row << g.lo, row << (g.lo + K1), row << (g.lo + K)};
+  const cuuint32_t box[5] = {C, 1, 1u << K1, 1u << K2, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 5, (void *)base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  ZKB_REQUIRE(r == CUDA_SUCCESS, "tensor map of an NTT pass refused (error %d)", (int)r);
+  return ZKB_OK;
+}
+
+template <int LR1, int LR2, int C>
+static int launch_pass_tma_c(const uint32_t *src, uint32_t *out, const PassGeom &g, uint32_t cols, uint64_t n_blocks,
+                             uint64_t ctas, const uint32_t *tw, uint32_t scale, const SmallTw<BabyBear> &st,
+                             cudaStream_t s) {
+  constexpr unsigned threads = C << LR2;
+  const size_t smem = tma_bar_off<LR1, LR2, C>() + 16;
+  CUtensorMap map;
+  ZKB_TRY(pass_tensor_map(&map, src, g, cols, LR1 + LR2, n_blocks, C));
+  ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_tma_kernel<LR1, LR2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024));
+  ZKB_LAUNCH("ntt_pass_tma", s, ntt_pass_tma_kernel<LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(src, out, g, tw, scale, st, map));
+  return ZKB_OK;
+}
+
 // Column segments of a `width`-column matrix: the widest chunk (at most cmax columns per
 // CTA) for the bulk, then narrower chunks (8, 4, 1) for what is left, each launched on
 // offset pointers with the full row stride.  Every width keeps coalesced rows for all
@@ -324,7 +419,18 @@ static int launch_pass_c(const typename F::T *src, typename F::T *out, const Pas
 template <class F, int LR1, int LR2>
 static int launch_pass(const typename F::T *src, typename F::T *out, const PassGeom &g, uint64_t ctas,
                        const typename F::T *tw, typename F::T scale, const SmallTw<F> &st,
-                       uint32_t C, cudaStream_t s) {
+                       uint32_t C, cudaStream_t s, uint32_t cols = 0, uint64_t n_blocks = 0) {
+  if constexpr (sizeof(typename F::T) == 4) {
+    // tensor-copy tile loads where every copy's start and the row stride are 16-byte aligned
+    if (cols && ntt_tile_loads().load() == 1 && C >= 4 && g.width % 4 == 0 && ((uintptr_t)src & 15) == 0) {
+      switch (C) {
+        case 16: return launch_pass_tma_c<LR1, LR2, 16>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
+        case 8: return launch_pass_tma_c<LR1, LR2, 8>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
+        case 4: return launch_pass_tma_c<LR1, LR2, 4>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
+        default: break;
+      }
+    }
+  }
   switch (C) {
     case 16:
       if constexpr (sizeof(typename F::T) == 4) return launch_pass_c<F, LR1, LR2, 16>(src, out, g, ctas, tw, scale, st, s);
@@ -387,19 +493,19 @@ static int run_plan(const typename F::T *in, typename F::T *out, int L, uint32_t
         return ZKB_ERR_UNSUPPORTED;
       }
       switch (K) {
-        case 1: rc = launch_pass<F, 1, 0>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 2: rc = launch_pass<F, 1, 1>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 3: rc = launch_pass<F, 2, 1>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 4: rc = launch_pass<F, 2, 2>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 5: rc = launch_pass<F, 3, 2>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 6: rc = launch_pass<F, 3, 3>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 7: rc = launch_pass<F, 4, 3>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 8: rc = launch_pass<F, 4, 4>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 9: rc = launch_pass<F, 5, 4>(sp, op, g, ctas, tw, scale, st, C, s); break;
-        case 10: rc = launch_pass<F, 5, 5>(sp, op, g, ctas, tw, scale, st, C, s); break;
+        case 1: rc = launch_pass<F, 1, 0>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 2: rc = launch_pass<F, 1, 1>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 3: rc = launch_pass<F, 2, 1>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 4: rc = launch_pass<F, 2, 2>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 5: rc = launch_pass<F, 3, 2>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 6: rc = launch_pass<F, 3, 3>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 7: rc = launch_pass<F, 4, 3>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 8: rc = launch_pass<F, 4, 4>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 9: rc = launch_pass<F, 5, 4>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
+        case 10: rc = launch_pass<F, 5, 5>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks); break;
         case 11:
           if constexpr (sizeof(T) == 4) {
-            rc = launch_pass<F, 6, 5>(sp, op, g, ctas, tw, scale, st, C, s);
+            rc = launch_pass<F, 6, 5>(sp, op, g, ctas, tw, scale, st, C, s, sg.cols, n_blocks);
             break;
           }
           [[fallthrough]];
@@ -681,5 +787,17 @@ template int ntt_lde_dev<BabyBear>(const uint32_t *, int, uint32_t, int, uint32_
                                    cudaStream_t, const LdeTune *, uint32_t *);
 template int ntt_lde_dev<Goldilocks>(const uint64_t *, int, uint32_t, int, uint64_t, bool,
                                      uint64_t *, cudaStream_t, const LdeTune *, uint64_t *);
+
+void set_ntt_tile_loads(int mode) { ntt_tile_loads().store(mode); }
+int ntt_tile_loads_mode() { return ntt_tile_loads().load(); }
+
+int ntt_tma_wait_errors(uint32_t *count) {
+  uint32_t v = 0;
+  ZKB_CHECK_CUDA(cudaMemcpyFromSymbol(&v, g_tma_wait_errors, sizeof v));
+  const uint32_t zero = 0;
+  ZKB_CHECK_CUDA(cudaMemcpyToSymbol(g_tma_wait_errors, &zero, sizeof zero));
+  *count = v;
+  return ZKB_OK;
+}
 
 }  // namespace zkb

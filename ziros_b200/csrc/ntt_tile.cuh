@@ -2,6 +2,7 @@
 // functions: the standalone kernels of ntt.cu run one tile per block, the persistent
 // batch kernel (persist.cu) runs them as work items.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -140,6 +141,48 @@ __device__ __forceinline__ void dif_reg(typename F::T (&x)[1 << LR], const Small
   });
 }
 
+// ---- tensor-copy (TMA) tile loads
+// A BabyBear pass tile can arrive in shared memory as ONE tensor copy (cp.async.bulk.tensor,
+// no multicast, this GPU's memory only) instead of R1 coalesced loads per thread: the
+// tensor map views a column segment as 5 dimensions (column, row bits below the pass,
+// the pass's bits in two parts of at most 8, the bits above it with the transform index)
+// and the box is C columns x 2^K rows, so row r of the tile lands at r * C.  Completion is
+// tracked by an mbarrier; every wait gives up after a bounded number of polls and raises an
+// error word instead of hanging.
+constexpr uint32_t TMA_WAIT_LIMIT = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// Polls the barrier's phase `parity` at most `limit` times; false when it never completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+  uint32_t done = 0;
+  for (uint32_t k = 0; k < limit && !done; k++)
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // Shared-memory geometry of a pass with C columns per CTA: f1 blocks of R2*C values,
 // padded so the stride is = C (mod 32) words and phase-B warps reading several f1
 // blocks hit distinct banks.
@@ -153,10 +196,14 @@ struct PassSmem {
 // runs inside the persistent batch kernel, whose blocks have more threads than the tile
 // uses (threads from C << LR2 up only stage twiddles and meet the barriers) and whose
 // inputs were written by other blocks of the same launch (read through L2, not L1).
-template <class F, int LR1, int LR2, int C, bool PERSIST>
+// TMA_IN: the tile's input rows are being copied into the start of shared memory (row r
+// at r * C) by a tensor copy that completes `bar`; phase A reads them there once it has
+// (a wait that gives up sets *err).
+template <class F, int LR1, int LR2, int C, bool PERSIST, bool TMA_IN = false>
 __device__ __forceinline__ void ntt_pass_tile(const typename F::T *in, typename F::T *out, const PassGeom &g,
                                               const typename F::T *__restrict__ tw, typename F::T post_scale,
-                                              const SmallTw<F> &st, uint32_t cta, unsigned char *smem_raw) {
+                                              const SmallTw<F> &st, uint32_t cta, unsigned char *smem_raw,
+                                              uint64_t *bar = nullptr, uint32_t *err = nullptr) {
   using T = typename F::T;
   constexpr int R1 = 1 << LR1, R2 = 1 << LR2, K = LR1 + LR2;
   constexpr int S = PassSmem<LR2, C>::STRIDE;
@@ -198,15 +245,22 @@ __device__ __forceinline__ void ntt_pass_tile(const typename F::T *in, typename 
   {
     T x[R1];
     if (active) {
-      const T *p = in + col0 + ((size_t)base_row * g.width) + (size_t)i * rs;
-      const size_t step = rs * R2;
+      if constexpr (TMA_IN) {
+        if (!mbar_wait(bar, 0, TMA_WAIT_LIMIT)) atomicExch(err, 1u);
+        const T *tp = sm + i * C + c;
 #pragma unroll
-      for (int j = 0; j < R1; j++) {
-        if constexpr (PERSIST)
-          x[j] = __ldcg(p);
-        else
-          x[j] = *p;
-        p += step;
+        for (int j = 0; j < R1; j++) x[j] = tp[j * R2 * C];
+      } else {
+        const T *p = in + col0 + ((size_t)base_row * g.width) + (size_t)i * rs;
+        const size_t step = rs * R2;
+#pragma unroll
+        for (int j = 0; j < R1; j++) {
+          if constexpr (PERSIST)
+            x[j] = __ldcg(p);
+          else
+            x[j] = *p;
+          p += step;
+        }
       }
       dif_reg<F, LR1>(x, st);
     }

@@ -115,9 +115,8 @@ struct zkb_engine {
   uint64_t budget = 0, in_use = 0;
   uint32_t policy = ZKB_ADMIT_FIFO;
   std::mutex mu;
-  // one trace piece crosses PCIe at a time, the fewest bytes left first; a piece passed
-  // over 64 times (16 GiB of other uploads) goes next — more than the 4.3 GB uploads of
-  // equal jobs submitted together, which keep uploading one after another
+  // one trace piece crosses PCIe at a time, the fewest bytes left first; an upload that 64
+  // pieces of later (smaller) uploads have passed over (16 GiB) goes next
   UploadGate upload_mu{64};
   // One job of each size class runs its LDE and tree at a time: equal jobs pipeline one's
   // upload under another's kernels instead of interleaving their kernels block by block;
