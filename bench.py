@@ -424,6 +424,8 @@ def load_traffic(workload: str):
 
 
 def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
+    import ctypes as C
+
     import numpy as np
     import torch
 
@@ -513,6 +515,38 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     e2e_lat = sorted(r[2]["latency_ms"] for r in res)
     engine.close()
 
+    # ---- the workload's LDE with each tile-load mode of the NTT kernels (tensor copies,
+    # the default, against coalesced loads into registers): best of 3 alternations of 5
+    # LDEs each, outputs compared
+    lde_out = torch.empty((n << lb, w), dtype=trace.dtype, device=dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    shift = 31 if field == 0 else 7
+    lde_ms, lde_ref = {}, None
+
+    def lde():
+        N.check(N.load().zkb_coset_lde_batch_dev(field, C.c_void_p(trace.data_ptr()), wl["log_h"], w, lb,
+                                                 C.c_uint64(shift), 1, C.c_void_p(lde_out.data_ptr()), sp))
+
+    for _ in range(3):
+        for mode, key in ((0, "registers_ms"), (1, "tensor_copy_ms")):
+            N.set_ntt_tile_loads(mode)
+            lde()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(5):
+                lde()
+            e1.record(stream)
+            e1.synchronize()
+            lde_ms[key] = min(lde_ms.get(key, 1e30), e0.elapsed_time(e1) / 5)
+            if lde_ref is None:
+                lde_ref = lde_out.clone()
+            else:
+                assert torch.equal(lde_ref, lde_out), "tile-load modes give different LDEs"
+    N.set_ntt_tile_loads(1)
+    assert N.ntt_tile_load_errors() == 0
+    del lde_out, lde_ref
+    torch.cuda.empty_cache()
+
     # ---- integer-multiply ceiling for the Poseidon2 roofline (measured, this GPU)
     mul_peak = N.measure_mul_peak(field)
 
@@ -555,20 +589,32 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     n_pass = -(-wl["log_h"] // kmax)
     b_blocks = 1 << lb
     ntt_roof = []
-    nk = kstats.get("ntt_pass")
+
+    def kstat(*names):
+        """(launches, total ms, max ms) summed over the kernels of these names (register or
+        tensor-copy tile loads)."""
+        got = [kstats[k] for k in names if k in kstats]
+        if not got:
+            return None
+        return (sum(g[0] for g in got), sum(g[1] for g in got), max(g[2] for g in got))
+
+    tile_loads = "tensor copy" if ("ntt_pass_tma" in kstats or "lde_fused_tma" in kstats) else "registers"
+    nk = kstat("ntt_pass", "ntt_pass_tma")
     if nk and n_pass > 1:
         bytes_per_step = 2 * esize * (n * w * (n_pass - 1) + N_rows * w * (n_pass - 1))
         per_launch = bytes_per_step * args.steps / nk[0]
         ach = per_launch / (nk[1] / nk[0] * 1e-3) / 1e9
-        ntt_roof.append({"kernel": "ntt_pass", "bound": "hbm", "unit": "GB/s", "achieved": ach, "peak": hbm_peak,
+        ntt_roof.append({"kernel": "ntt_pass", "tile_loads": tile_loads, "bound": "hbm", "unit": "GB/s",
+                         "achieved": ach, "peak": hbm_peak,
                          "frac": ach / hbm_peak, "peak_source": hbm_src,
                          "algorithmic_bytes_per_launch": per_launch,
                          "traffic": traffic.get("ntt_pass") if traffic else None})
-    fk = kstats.get("lde_fused")
+    fk = kstat("lde_fused", "lde_fused_tma")
     if fk:
         per_launch = esize * (n * w + b_blocks * n * w)
         ach = per_launch / (fk[1] / fk[0] * 1e-3) / 1e9
-        ntt_roof.append({"kernel": "lde_fused", "bound": "hbm", "unit": "GB/s", "achieved": ach, "peak": hbm_peak,
+        ntt_roof.append({"kernel": "lde_fused", "tile_loads": tile_loads, "bound": "hbm", "unit": "GB/s",
+                         "achieved": ach, "peak": hbm_peak,
                          "frac": ach / hbm_peak, "peak_source": hbm_src,
                          "algorithmic_bytes_per_launch": per_launch,
                          "traffic": traffic.get("lde_fused") if traffic else None})
@@ -609,6 +655,8 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         "parity": parity,
         "roofline": roofline,
         "roofline_ntt": ntt_roof,
+        "lde_tile_loads": dict({k: round(v, 3) for k, v in lde_ms.items()},
+                               what="the workload's coset LDE alone (zkb_coset_lde_batch_dev), best of 3 x 5"),
         "step": "LDE + Poseidon2 MMCS" + (" + alpha-reduction + FRI (2^%d -> 2^%d, %d queries)" % (
             wl["log_h"] + lb, FRI["log_final"], FRI["num_queries"]) if with_fri else ""),
         "cpu_baseline": cpu,

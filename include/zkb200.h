@@ -172,15 +172,16 @@ ZKB_API int zkb_dft_batch_dev(int field, void *d_rowmajor, uint32_t log_h, uint3
 ZKB_API int zkb_dft_batch_noalloc_dev(int field, void *d_rowmajor, uint32_t log_h, uint32_t width,
                                       int inverse, void *stream);
 
-/* Tile loads of the BabyBear NTT passes (DFT, LDE, commits; process-wide): 0 = coalesced
- * loads straight into registers (the default); 1 = one tensor copy (TMA,
- * cp.async.bulk.tensor, no multicast) of each pass tile into shared memory, used where the
- * rows are 16-byte aligned (width a multiple of 4, column chunks of 4 or more; other passes
- * keep the loads).  ZKB_NTT_TMA=1 in the environment selects 1 at load.  Results are the
- * same bit for bit.  No counterpart in the reference. */
+/* Tile loads of the NTT passes and the fused LDE middle (DFT, LDE, commits;
+ * process-wide): 1 = one tensor copy (TMA, cp.async.bulk.tensor, no multicast) of each
+ * tile into shared memory (the default), used where the row stride and the column chunk
+ * are multiples of 16 bytes (BabyBear: width a multiple of 4, chunks of 4 columns or more;
+ * Goldilocks: even width, chunks of 4 or 8; other tiles keep the loads); 0 = coalesced
+ * loads straight into registers.  ZKB_NTT_TMA=0 in the environment selects 0 at load.
+ * Results are the same bit for bit.  No counterpart in the reference. */
 ZKB_API int zkb_set_ntt_tile_loads(int mode);
-/* Tensor-copy waits of the NTT passes that gave up (bounded polls) since the last call;
- * nonzero means those passes' outputs are invalid.  Resets the count. */
+/* Tensor-copy waits of the NTT tiles that gave up (bounded polls) since the last call;
+ * nonzero means those outputs are invalid.  Resets the count. */
 ZKB_API int zkb_ntt_tile_load_errors(uint32_t *count);
 
 /* p3 coset_lde_batch(trace, log_blowup, shift) followed, when bitrev_rows=1, by

@@ -276,7 +276,7 @@ def release_cached_memory() -> None:
 
 
 def set_ntt_tile_loads(mode: int) -> None:
-    """BabyBear NTT pass tiles: 0 = loads into registers (default), 1 = one tensor copy per tile."""
+    """NTT tiles: 1 = one tensor copy per tile (default), 0 = coalesced loads into registers."""
     check(load().zkb_set_ntt_tile_loads(int(mode)))
 
 

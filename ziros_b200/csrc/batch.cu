@@ -291,17 +291,18 @@ struct zkb_batch {
   }
 
   // A run whose traces come from host memory, the copies overlapped with the commitment:
-  // the copy stream takes the traces smallest first, in groups (consecutive in that order,
-  // growing from about 1/64 of the batch's cells to at most 1/16; a larger trace is a group
-  // by itself), and each group's LDEs and trees run on origin as soon as its last copy has
-  // landed, while the next groups copy.  A trace's commitment takes longer than its copy at
-  // any size (the rates are near proportional), so smallest first is Johnson's order for a
-  // two-stage flow (copy, then compute): compute starts after the first, small group's copy
-  // and is not left waiting after that, and the last group, whose compute follows the last
-  // copy, is at most one large trace or 1/16 of the batch.  Copies and launches are
-  // enqueued group by group, so a pageable source (staged by the copy call) still overlaps
-  // the staging of later groups with the work on earlier ones.  A persistent plan reads
-  // every trace from its one kernel: its copies all go first.
+  // the copy stream takes the traces in groups (about 1/64 of the batch's cells each, a
+  // larger trace by itself), and each group's LDEs and trees run on origin as soon as its
+  // last copy has landed, while the next groups copy.  This is a two-stage flow (copy, then
+  // compute) whose two stages run at similar rates per cell (the compute a little slower
+  // or faster, depending on the host link): the work done outside the overlap is the
+  // first group's copy and the last group's compute, so the copy order puts small traces
+  // at both ends and the largest in the middle, growing gradually on the way up (a copy
+  // then rarely outlasts the compute of the group before it) and shrinking on the way
+  // down.  Copies and launches are enqueued group by group, so a pageable source (staged
+  // by the copy call) still overlaps the staging of later groups with the work on earlier
+  // ones.  A persistent plan reads every trace from its one kernel: its copies all go
+  // first.
   int run_host(const void *const *src, cudaStream_t origin) {
     const size_t n = shapes.size();
     for (size_t i = 0; i < n; i++) ZKB_REQUIRE(src[i] != nullptr, "trace %zu: null host source", i);
@@ -796,32 +797,34 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
     b->joint.comp = c;
     b->joint.root_off = r;
   }
-  // host groups: traces by cells, fewest first; a group closes once it holds `target`
-  // cells (about 1/64 of the batch, doubling per group up to 1/16) or before a trace
-  // that would take it past that; a larger trace forms a group by itself
+  // host groups: the copy order puts the small traces at both ends and the largest in
+  // the middle (sorted by cells: the even positions ascending, then the odd ones
+  // descending); a group closes once it holds `target` cells (1/64 of the batch, at least
+  // 2^23) or before a trace that would take it past that; a larger trace forms a group by
+  // itself
   std::vector<char> img;
   if (!b->persistent) {
     auto cells = [&](int i) { return (uint64_t)b->shapes[i].width << b->shapes[i].log_h; };
-    std::vector<int> ord(n);
-    std::iota(ord.begin(), ord.end(), 0);
-    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cells(x) < cells(y); });
+    std::vector<int> sorted(n), ord;
+    std::iota(sorted.begin(), sorted.end(), 0);
+    std::stable_sort(sorted.begin(), sorted.end(), [&](int x, int y) { return cells(x) < cells(y); });
+    for (size_t k = 0; k < n; k += 2) ord.push_back(sorted[k]);
+    for (size_t k = (n % 2 ? n - 2 : n - 1); k < n; k -= 2) ord.push_back(sorted[k]);
     uint64_t total = 0;
     for (size_t i = 0; i < n; i++) total += cells((int)i);
-    const uint64_t cap = std::max<uint64_t>(total / 16, 1);
-    uint64_t target = std::min<uint64_t>(cap, std::max<uint64_t>(total / 64, 1ull << 20)), acc = 0;
+    const uint64_t target = std::max<uint64_t>(total / 64, 1ull << 23);
+    uint64_t acc = 0;
     std::vector<std::vector<int>> groups(1);
     for (int i : ord) {
       if (!groups.back().empty() && acc + cells(i) > target) {
         groups.emplace_back();
         acc = 0;
-        target = std::min(cap, 2 * target);
       }
       groups.back().push_back(i);
       acc += cells(i);
       if (acc >= target) {
         groups.emplace_back();
         acc = 0;
-        target = std::min(cap, 2 * target);
       }
     }
     if (groups.back().empty()) groups.pop_back();

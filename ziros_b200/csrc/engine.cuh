@@ -133,8 +133,8 @@ struct FriProof {
   ~FriProof();
 };
 
-// Tile loads of the BabyBear NTT passes (0 = coalesced loads into registers, 1 = one
-// tensor copy per tile), and the count of tensor-copy waits that gave up (reset on read).
+// Tile loads of the NTT passes (0 = coalesced loads into registers, 1 = one tensor copy
+// per tile), and the count of tensor-copy waits that gave up (reset on read).
 void set_ntt_tile_loads(int mode);
 int ntt_tile_loads_mode();
 int ntt_tma_wait_errors(uint32_t *count);

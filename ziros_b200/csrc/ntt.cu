@@ -264,44 +264,46 @@ __global__ void __launch_bounds__(C << LR2)
   ntt_pass_tile<F, LR1, LR2, C, false>(in, out, g, tw, post_scale, st, blockIdx.x, smem_raw);
 }
 
-// The same pass with its tile brought in by one tensor copy (BabyBear; see ntt_tile.cuh).
-// Thread 0 sets up the barrier and issues the copy, which runs while the block stages its
+// The same pass with its tile brought in by one tensor copy (see ntt_tile.cuh).  Thread 0
+// sets up the barrier and issues the copy, which runs while the block stages its
 // twiddles.
-template <int LR1, int LR2, int C>
+template <class F, int LR1, int LR2, int C>
 constexpr size_t tma_bar_off() {
-  return (pass_tile_smem<BabyBear, LR1, LR2, C>() + 15) & ~(size_t)15;
+  return (pass_tile_smem<F, LR1, LR2, C>() + 15) & ~(size_t)15;
 }
 
 __device__ uint32_t g_tma_wait_errors;
 
-template <int LR1, int LR2, int C>
+template <class F, int LR1, int LR2, int C>
 __global__ void __launch_bounds__(C << LR2)
-    ntt_pass_tma_kernel(const uint32_t *in, uint32_t *out, const PassGeom g, const uint32_t *__restrict__ tw,
-                        uint32_t post_scale, const __grid_constant__ SmallTw<BabyBear> st,
-                        const __grid_constant__ CUtensorMap map) {
+    ntt_pass_tma_kernel(const typename F::T *in, typename F::T *out, const PassGeom g,
+                        const typename F::T *__restrict__ tw, typename F::T post_scale,
+                        const __grid_constant__ SmallTw<F> st, const __grid_constant__ CUtensorMap map) {
   extern __shared__ __align__(128) unsigned char tma_smem[];  // the tensor copy's destination
   constexpr int K = LR1 + LR2;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(tma_smem + tma_bar_off<LR1, LR2, C>());
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tma_smem + tma_bar_off<F, LR1, LR2, C>());
   if (threadIdx.x == 0) {
     const uint32_t chunk = blockIdx.x % g.chunks_per_row, rest = blockIdx.x / g.chunks_per_row;
     const uint32_t grp = rest % g.groups, blk = rest / g.groups;
     const uint32_t i_low = grp & ((1u << g.lo) - 1u);
     const uint32_t high = blk * (g.groups >> g.lo) + (grp >> g.lo);  // row bits above the pass, transform
     mbar_init(bar, 1);
-    mbar_expect_tx(bar, (uint32_t)(C << K) * 4u);
+    mbar_expect_tx(bar, (uint32_t)((C << K) * sizeof(typename F::T)));
     tma_load_5d(tma_smem, &map, bar, (int)(chunk * C), (int)i_low, 0, 0, (int)high);
   }
   __syncthreads();  // the barrier is initialised before anyone waits on it
-  ntt_pass_tile<BabyBear, LR1, LR2, C, false, true>(in, out, g, tw, post_scale, st, blockIdx.x, tma_smem, bar,
-                                                    &g_tma_wait_errors);
+  ntt_pass_tile<F, LR1, LR2, C, false, true>(in, out, g, tw, post_scale, st, blockIdx.x, tma_smem, bar,
+                                             &g_tma_wait_errors);
 }
 
-// Tile loads of the BabyBear passes: 0 = coalesced loads into registers (the default),
-// 1 = one tensor copy per tile.  Set by zkb_set_ntt_tile_loads or ZKB_NTT_TMA=1.
+// Tile loads of the passes and the fused middle: 1 = one tensor copy per tile (the
+// default; measured 2-11 % faster than register loads on BabyBear and Goldilocks LDEs of
+// 2^18..2^22 rows), 0 = coalesced loads into registers.  Set by zkb_set_ntt_tile_loads or
+// ZKB_NTT_TMA=0/1.
 std::atomic<int> &ntt_tile_loads() {
   static std::atomic<int> mode{[] {
     const char *v = getenv("ZKB_NTT_TMA");
-    return v && *v == '1' ? 1 : 0;
+    return v && *v == '0' ? 0 : 1;
   }()};
   return mode;
 }
@@ -321,39 +323,41 @@ static EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// Tensor map of one column segment (`cols` columns from `base`, row stride g.width) for the
-// tiles of a K-bit pass at bits [g.lo, g.lo + K): dimensions (column, row bits below the
-// pass, the pass's bits split 8 + rest, the bits above with the transform index), box C
-// columns x 2^K rows.  The caller has checked: 4-byte elements, width % 4 == 0, base
-// 16-byte aligned, C >= 4 (every copy starts at a column that is a multiple of C).
-static int pass_tensor_map(CUtensorMap *m, const uint32_t *base, const PassGeom &g, uint32_t cols, int K,
+// Tensor map of one column segment (`cols` columns of `es`-byte elements from `base`, row
+// stride g.width) for the tiles of a K-bit pass at bits [g.lo, g.lo + K): dimensions
+// (column, row bits below the pass, the pass's bits split 8 + rest, the bits above with
+// the transform index), box C columns x 2^K rows.  The caller has checked that the row
+// stride, the base and C * es are multiples of 16 bytes (every copy starts at a column
+// that is a multiple of C).
+static int pass_tensor_map(CUtensorMap *m, const void *base, size_t es, const PassGeom &g, uint32_t cols, int K,
                            uint64_t n_blocks, uint32_t C) {
   const EncodeTiledFn fn = encode_tiled();
   ZKB_REQUIRE(fn != nullptr, "cuTensorMapEncodeTiled is not available");
   const int K1 = K < 8 ? K : 8, K2 = K - K1;
-  const uint64_t row = (uint64_t)g.width * 4;
+  const uint64_t row = (uint64_t)g.width * es;
   const cuuint64_t dims[5] = {cols, 1ull << g.lo, 1ull << K1, 1ull << K2, (1ull << (g.L - g.lo - K)) * n_blocks};
   const cuuint64_t strides[4] = {row, row << g.lo, row << (g.lo + K1), row << (g.lo + K)};
   const cuuint32_t box[5] = {C, 1, 1u << K1, 1u << K2, 1};
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 5, (void *)base, dims, strides, box, estr,
+  const CUresult r = fn(m, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, (void *)base,
+                        dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   ZKB_REQUIRE(r == CUDA_SUCCESS, "tensor map of an NTT pass refused (error %d)", (int)r);
   return ZKB_OK;
 }
 
-template <int LR1, int LR2, int C>
-static int launch_pass_tma_c(const uint32_t *src, uint32_t *out, const PassGeom &g, uint32_t cols, uint64_t n_blocks,
-                             uint64_t ctas, const uint32_t *tw, uint32_t scale, const SmallTw<BabyBear> &st,
-                             cudaStream_t s) {
+template <class F, int LR1, int LR2, int C>
+static int launch_pass_tma_c(const typename F::T *src, typename F::T *out, const PassGeom &g, uint32_t cols,
+                             uint64_t n_blocks, uint64_t ctas, const typename F::T *tw, typename F::T scale,
+                             const SmallTw<F> &st, cudaStream_t s) {
   constexpr unsigned threads = C << LR2;
-  const size_t smem = tma_bar_off<LR1, LR2, C>() + 16;
+  const size_t smem = tma_bar_off<F, LR1, LR2, C>() + 16;
   CUtensorMap map;
-  ZKB_TRY(pass_tensor_map(&map, src, g, cols, LR1 + LR2, n_blocks, C));
-  ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_tma_kernel<LR1, LR2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      200 * 1024));
-  ZKB_LAUNCH("ntt_pass_tma", s, ntt_pass_tma_kernel<LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(src, out, g, tw, scale, st, map));
+  ZKB_TRY(pass_tensor_map(&map, src, sizeof(typename F::T), g, cols, LR1 + LR2, n_blocks, C));
+  ZKB_CHECK_CUDA(cudaFuncSetAttribute(ntt_pass_tma_kernel<F, LR1, LR2, C>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  ZKB_LAUNCH("ntt_pass_tma", s, ntt_pass_tma_kernel<F, LR1, LR2, C><<<(unsigned)ctas, threads, smem, s>>>(src, out, g, tw, scale, st, map));
   return ZKB_OK;
 }
 
@@ -420,15 +424,17 @@ template <class F, int LR1, int LR2>
 static int launch_pass(const typename F::T *src, typename F::T *out, const PassGeom &g, uint64_t ctas,
                        const typename F::T *tw, typename F::T scale, const SmallTw<F> &st,
                        uint32_t C, cudaStream_t s, uint32_t cols = 0, uint64_t n_blocks = 0) {
-  if constexpr (sizeof(typename F::T) == 4) {
-    // tensor-copy tile loads where every copy's start and the row stride are 16-byte aligned
-    if (cols && ntt_tile_loads().load() == 1 && C >= 4 && g.width % 4 == 0 && ((uintptr_t)src & 15) == 0) {
-      switch (C) {
-        case 16: return launch_pass_tma_c<LR1, LR2, 16>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
-        case 8: return launch_pass_tma_c<LR1, LR2, 8>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
-        case 4: return launch_pass_tma_c<LR1, LR2, 4>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
-        default: break;
-      }
+  // tensor-copy tile loads where every copy's start and the row stride are 16-byte aligned
+  constexpr size_t es = sizeof(typename F::T);
+  if (cols && ntt_tile_loads().load() == 1 && C * es >= 16 && (g.width * es) % 16 == 0 &&
+      ((uintptr_t)src & 15) == 0) {
+    switch (C) {
+      case 16:
+        if constexpr (es == 4) return launch_pass_tma_c<F, LR1, LR2, 16>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
+        break;
+      case 8: return launch_pass_tma_c<F, LR1, LR2, 8>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
+      case 4: return launch_pass_tma_c<F, LR1, LR2, 4>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
+      default: break;
     }
   }
   switch (C) {
@@ -542,12 +548,56 @@ __global__ void __launch_bounds__(C << LR2)
   lde_fused_tile<F, LR1, LR2, C, false>(in, out, g, itw, ftw, ctab_t, ftw_t, ist, fst, blockIdx.x, smem_raw);
 }
 
+// The fused middle with block B's rows brought in by one tensor copy (as the passes).
+template <class F, int LR1, int LR2, int C>
+constexpr size_t fused_bar_off() {
+  return (fused_tile_smem<F, LR1, LR2, C>() + 15) & ~(size_t)15;
+}
+
+template <class F, int LR1, int LR2, int C>
+__global__ void __launch_bounds__(C << LR2)
+    lde_fused_tma_kernel(const typename F::T *in, typename F::T *out, const FusedGeom g,
+                         const typename F::T *__restrict__ itw, const typename F::T *__restrict__ ftw,
+                         const typename F::T *__restrict__ ctab_t, const typename F::T *__restrict__ ftw_t,
+                         const __grid_constant__ SmallTw<F> ist, const __grid_constant__ SmallTw<F> fst,
+                         const __grid_constant__ CUtensorMap map) {
+  extern __shared__ __align__(128) unsigned char tma_smem[];
+  constexpr int K = LR1 + LR2;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tma_smem + fused_bar_off<F, LR1, LR2, C>());
+  if (threadIdx.x == 0) {
+    const uint32_t chunk = blockIdx.x % g.chunks_per_row, B = blockIdx.x / g.chunks_per_row;
+    mbar_init(bar, 1);
+    mbar_expect_tx(bar, (uint32_t)((C << K) * sizeof(typename F::T)));
+    tma_load_5d(tma_smem, &map, bar, (int)(chunk * C), 0, 0, 0, (int)B);
+  }
+  __syncthreads();  // the barrier is initialised before anyone waits on it
+  lde_fused_tile<F, LR1, LR2, C, false, true>(in, out, g, itw, ftw, ctab_t, ftw_t, ist, fst, blockIdx.x, tma_smem,
+                                              bar, &g_tma_wait_errors);
+}
+
 template <class F, int LR1, int LR2, int C>
 static int launch_fused_c(const typename F::T *in, typename F::T *out, const FusedGeom &g,
                           const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
-                          const typename F::T *ftw_t, cudaStream_t s) {
+                          const typename F::T *ftw_t, cudaStream_t s, uint32_t cols) {
   using T = typename F::T;
   constexpr unsigned threads = C << LR2;
+  const uint64_t ctas0 = (uint64_t)g.chunks_per_row * g.blocks;
+  if (cols && ntt_tile_loads().load() == 1 && C * sizeof(T) >= 16 && (g.width * sizeof(T)) % 16 == 0 &&
+      ((uintptr_t)in & 15) == 0) {
+    // block B's rows as the tile of a pass at bits [0, K) of one transform
+    PassGeom pg;
+    pg.L = g.L;
+    pg.lo = 0;
+    pg.width = g.width;
+    CUtensorMap map;
+    ZKB_TRY(pass_tensor_map(&map, in, sizeof(T), pg, cols, LR1 + LR2, 1, C));
+    const size_t smem = fused_bar_off<F, LR1, LR2, C>() + 16;
+    ZKB_CHECK_CUDA(cudaFuncSetAttribute(lde_fused_tma_kernel<F, LR1, LR2, C>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    const SmallTw<F> ist = small_twiddles<F>(true), fst = small_twiddles<F>(false);
+    ZKB_LAUNCH("lde_fused_tma", s, lde_fused_tma_kernel<F, LR1, LR2, C><<<(unsigned)ctas0, threads, smem, s>>>(in, out, g, itw, ftw, ctab, ftw_t, ist, fst, map));
+    return ZKB_OK;
+  }
   const size_t smem = fused_tile_smem<F, LR1, LR2, C>();
   ZKB_CHECK_CUDA(cudaFuncSetAttribute(lde_fused_kernel<F, LR1, LR2, C>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -562,11 +612,11 @@ static int launch_fused_c(const typename F::T *in, typename F::T *out, const Fus
 template <class F, int LR1, int LR2>
 static int launch_fused(const typename F::T *in, typename F::T *out, const FusedGeom &g,
                         const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
-                        const typename F::T *ftw_t, uint32_t C, cudaStream_t s) {
+                        const typename F::T *ftw_t, uint32_t C, cudaStream_t s, uint32_t cols) {
   switch (C) {
-    case 8: return launch_fused_c<F, LR1, LR2, 8>(in, out, g, itw, ftw, ctab, ftw_t, s);
-    case 4: return launch_fused_c<F, LR1, LR2, 4>(in, out, g, itw, ftw, ctab, ftw_t, s);
-    case 1: return launch_fused_c<F, LR1, LR2, 1>(in, out, g, itw, ftw, ctab, ftw_t, s);
+    case 8: return launch_fused_c<F, LR1, LR2, 8>(in, out, g, itw, ftw, ctab, ftw_t, s, cols);
+    case 4: return launch_fused_c<F, LR1, LR2, 4>(in, out, g, itw, ftw, ctab, ftw_t, s, cols);
+    case 1: return launch_fused_c<F, LR1, LR2, 1>(in, out, g, itw, ftw, ctab, ftw_t, s, cols);
     default: break;
   }
   set_error("internal: fused LDE column chunk %u", C);
@@ -625,20 +675,20 @@ int ntt_dft_dev(typename F::T *d, int log_h, uint32_t width, bool inverse, cudaS
 template <class F>
 static int launch_fused_k(int K, const typename F::T *in, typename F::T *out, const FusedGeom &g,
                           const typename F::T *itw, const typename F::T *ftw, const typename F::T *ctab,
-                          const typename F::T *ftw_t, uint32_t C, cudaStream_t s) {
+                          const typename F::T *ftw_t, uint32_t C, cudaStream_t s, uint32_t cols) {
   switch (K) {
-    case 1: return launch_fused<F, 1, 0>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 2: return launch_fused<F, 1, 1>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 3: return launch_fused<F, 2, 1>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 4: return launch_fused<F, 2, 2>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 5: return launch_fused<F, 3, 2>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 6: return launch_fused<F, 3, 3>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 7: return launch_fused<F, 4, 3>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 8: return launch_fused<F, 4, 4>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 9: return launch_fused<F, 5, 4>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
-    case 10: return launch_fused<F, 5, 5>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+    case 1: return launch_fused<F, 1, 0>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 2: return launch_fused<F, 1, 1>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 3: return launch_fused<F, 2, 1>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 4: return launch_fused<F, 2, 2>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 5: return launch_fused<F, 3, 2>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 6: return launch_fused<F, 3, 3>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 7: return launch_fused<F, 4, 3>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 8: return launch_fused<F, 4, 4>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 9: return launch_fused<F, 5, 4>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
+    case 10: return launch_fused<F, 5, 5>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
     case 11:
-      if constexpr (sizeof(typename F::T) == 4) return launch_fused<F, 6, 5>(in, out, g, itw, ftw, ctab, ftw_t, C, s);
+      if constexpr (sizeof(typename F::T) == 4) return launch_fused<F, 6, 5>(in, out, g, itw, ftw, ctab, ftw_t, C, s, cols);
       [[fallthrough]];
     default:
       set_error("internal: fused LDE pass of %d bits", K);
@@ -726,7 +776,7 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
         set_error("LDE launch too large");
         return ZKB_ERR_UNSUPPORTED;
       }
-      ZKB_TRY(launch_fused_k<F>(Kf, src + sg.col0, d_out + sg.col0, g, itw, ftw, ctab_t, ftw_t, sg.C, s));
+      ZKB_TRY(launch_fused_k<F>(Kf, src + sg.col0, d_out + sg.col0, g, itw, ftw, ctab_t, ftw_t, sg.C, s, sg.cols));
     }
     std::vector<int> tail(ks.rbegin() + 1, ks.rend());
     if (!tail.empty())

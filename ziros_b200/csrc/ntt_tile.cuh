@@ -142,7 +142,7 @@ __device__ __forceinline__ void dif_reg(typename F::T (&x)[1 << LR], const Small
 }
 
 // ---- tensor-copy (TMA) tile loads
-// A BabyBear pass tile can arrive in shared memory as ONE tensor copy (cp.async.bulk.tensor,
+// A pass tile can arrive in shared memory as ONE tensor copy (cp.async.bulk.tensor,
 // no multicast, this GPU's memory only) instead of R1 coalesced loads per thread: the
 // tensor map views a column segment as 5 dimensions (column, row bits below the pass,
 // the pass's bits in two parts of at most 8, the bits above it with the transform index)
@@ -322,14 +322,16 @@ struct FusedGeom {
   uint64_t n;        // 2^L
 };
 
-// One CTA-tile of the fused LDE middle (tile index `cta`); PERSIST as for ntt_pass_tile.
-template <class F, int LR1, int LR2, int C, bool PERSIST>
+// One CTA-tile of the fused LDE middle (tile index `cta`); PERSIST and TMA_IN as for
+// ntt_pass_tile (the tensor copy brings the 2^K rows of block B).
+template <class F, int LR1, int LR2, int C, bool PERSIST, bool TMA_IN = false>
 __device__ __forceinline__ void lde_fused_tile(const typename F::T *in, typename F::T *out, const FusedGeom &g,
                                                const typename F::T *__restrict__ itw,
                                                const typename F::T *__restrict__ ftw,
                                                const typename F::T *__restrict__ ctab_t,
                                                const typename F::T *__restrict__ ftw_t, const SmallTw<F> &ist,
-                                               const SmallTw<F> &fst, uint32_t cta, unsigned char *smem_raw) {
+                                               const SmallTw<F> &fst, uint32_t cta, unsigned char *smem_raw,
+                                               uint64_t *bar = nullptr, uint32_t *err = nullptr) {
   using T = typename F::T;
   constexpr int R1 = 1 << LR1, R2 = 1 << LR2, K = LR1 + LR2, Q = R1 / R2;
   constexpr int S = PassSmem<LR2, C>::STRIDE;
@@ -363,15 +365,22 @@ __device__ __forceinline__ void lde_fused_tile(const typename F::T *in, typename
   {
     T x[R1];
     if (active) {
-      const T *p = in + colc + ((size_t)B * (1u << K) + i) * g.width;
-      const size_t step = (size_t)R2 * g.width;
+      if constexpr (TMA_IN) {
+        if (!mbar_wait(bar, 0, TMA_WAIT_LIMIT)) atomicExch(err, 1u);
+        const T *tp = sm + i * C + c;
 #pragma unroll
-      for (int j = 0; j < R1; j++) {
-        if constexpr (PERSIST)
-          x[j] = __ldcg(p);
-        else
-          x[j] = *p;
-        p += step;
+        for (int j = 0; j < R1; j++) x[j] = tp[j * R2 * C];
+      } else {
+        const T *p = in + colc + ((size_t)B * (1u << K) + i) * g.width;
+        const size_t step = (size_t)R2 * g.width;
+#pragma unroll
+        for (int j = 0; j < R1; j++) {
+          if constexpr (PERSIST)
+            x[j] = __ldcg(p);
+          else
+            x[j] = *p;
+          p += step;
+        }
       }
       dif_reg<F, LR1>(x, ist);
     }
