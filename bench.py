@@ -61,6 +61,10 @@ WORKLOADS = {
     # many small traces (launch-bound as plain calls): 256 traces, log2 rows in [8, 14], widths {8..64}
     "batch256_small_babybear": dict(kind="batch", field=0, n=256, log_h_lo=8, log_h_hi=14, w_step=8, w_hi=64,
                                     log_blowup=1, p2w=16, seed=9, width=36, log_h=14),
+    # the coset LDE alone under both tile-load modes of the NTT kernels (tensor copies, the
+    # default, and coalesced loads into registers): (field, log_h, width, log_blowup)
+    "lde_tile_loads": dict(kind="lde_sweep", field=0, log_h=22, width=256, log_blowup=1, p2w=16,
+                           shapes=[(0, 22, 256, 1), (1, 20, 64, 2), (0, 20, 64, 1), (0, 18, 256, 1)]),
 }
 DEFAULT_WORKLOAD = "babybear_2^22x256_b2"
 P2_SEED = 42
@@ -1109,6 +1113,69 @@ def run_serving(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
     return 0
 
 
+def run_lde_sweep(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
+    """The coset LDE (zkb_coset_lde_batch_dev, rows bit-reversed) of each shape under both
+    tile-load modes of the NTT kernels, alternating the modes: best of `steps` rounds of 10
+    LDEs each after `warmup` untimed ones; the outputs of the two modes are compared."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from ziros_b200 import _native as N
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = N.load()
+    N.check(lib.zkb_set_device(local_rank))
+    stream = torch.cuda.current_stream(dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    out_rows = []
+    for field, log_h, w, lb in wl["shapes"]:
+        n = 1 << log_h
+        t = fill_uniform(torch, field, (n, w), TRACE_SEED, dev)
+        out = torch.empty((n << lb, w), dtype=t.dtype, device=dev)
+        shift = 31 if field == 0 else 7
+
+        def lde():
+            N.check(lib.zkb_coset_lde_batch_dev(field, C.c_void_p(t.data_ptr()), log_h, w, lb, C.c_uint64(shift), 1,
+                                                C.c_void_p(out.data_ptr()), sp))
+
+        best, ref = {}, None
+        for _ in range(max(args.steps, 1)):
+            for mode, key in ((0, "registers_ms"), (1, "tensor_copy_ms")):
+                N.set_ntt_tile_loads(mode)
+                for _ in range(max(args.warmup, 1)):
+                    lde()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(10):
+                    lde()
+                e1.record(stream)
+                e1.synchronize()
+                best[key] = min(best.get(key, 1e30), e0.elapsed_time(e1) / 10)
+                if ref is None:
+                    ref = out.clone()
+                else:
+                    assert torch.equal(ref, out), "tile-load modes give different LDEs"
+        N.set_ntt_tile_loads(1)
+        out_rows.append(dict(field="babybear" if field == 0 else "goldilocks", log_h=log_h, width=w, log_blowup=lb,
+                             registers_ms=round(best["registers_ms"], 4),
+                             tensor_copy_ms=round(best["tensor_copy_ms"], 4),
+                             speedup=round(best["registers_ms"] / best["tensor_copy_ms"], 4)))
+        del t, out, ref
+        torch.cuda.empty_cache()
+    assert N.ntt_tile_load_errors() == 0
+    if rank == 0:
+        speed = [r["speedup"] for r in out_rows]
+        gm = float(np.exp(np.mean(np.log(speed))))
+        print(json.dumps({"metric": "coset LDE time, tensor-copy vs register tile loads (geometric-mean speed-up)",
+                          "value": gm, "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                          "higher_is_better": True, "vs_baseline": None, "data": "synthetic (seeded uniform)",
+                          "config": {"workload": args.workload}, "shapes": out_rows}), flush=True)
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -1130,6 +1197,8 @@ def main() -> int:
         return run_batch(args, wl, rank, world, local_rank)
     if wl.get("kind") == "serving":
         return run_serving(args, wl, rank, world, local_rank)
+    if wl.get("kind") == "lde_sweep":
+        return run_lde_sweep(args, wl, rank, world, local_rank)
     if args.sharded:
         return run_sharded(args, wl, rank, world, local_rank)
     return run_ours(args, wl, rank, world, local_rank)

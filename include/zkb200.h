@@ -551,10 +551,11 @@ ZKB_API int zkb_batch_copy_in(zkb_batch *batch, size_t i, const void *src, int s
 ZKB_API int zkb_batch_run(zkb_batch *batch, void *stream);
 /* One run whose traces come from host memory: traces[i] points to trace i (2^log_h x width,
  * row-major, canonical elements; pinned host memory for the copies to run asynchronously).
- * The copies overlap the commitment: one copy stream takes the traces smallest first, and
- * each trace's LDE and its own tree start on its branch as soon as its copy has landed
- * (per-trace tree launches instead of the graph's joint ones).  A persistent
- * plan copies every trace first, then runs its kernel.  Pinned sources are read until
+ * The copies overlap the commitment: a copy stream takes the traces in groups (about 1/64
+ * of the batch's cells each, small traces first and last, the largest in the middle), and
+ * each group's LDEs and trees — one graph per group, captured at creation — run on `stream`
+ * as soon as the group's copies have landed.  A persistent plan copies every trace first,
+ * then runs its kernel.  Pinned sources are read until
  * `stream` has passed the run; pageable ones are staged before the call returns.  Roots
  * and trees as after zkb_batch_run.  No counterpart in the reference. */
 ZKB_API int zkb_batch_run_host(zkb_batch *batch, const void *const *traces, void *stream);
