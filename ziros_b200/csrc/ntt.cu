@@ -297,8 +297,8 @@ __global__ void __launch_bounds__(C << LR2)
 }
 
 // Tile loads of the passes and the fused middle: 1 = one tensor copy per tile (the
-// default; measured 2-11 % faster than register loads on BabyBear and Goldilocks LDEs of
-// 2^18..2^22 rows), 0 = coalesced loads into registers.  Set by zkb_set_ntt_tile_loads or
+// default; measured 0.6-12.5 % faster than register loads on BabyBear and Goldilocks LDEs
+// of 2^18..2^22 rows), 0 = coalesced loads into registers.  Set by zkb_set_ntt_tile_loads or
 // ZKB_NTT_TMA=0/1.
 std::atomic<int> &ntt_tile_loads() {
   static std::atomic<int> mode{[] {
