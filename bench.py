@@ -477,15 +477,18 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
                              host_ptr=pinned.data_ptr(), shape=(n, w)) for _ in range(k)]
         return [engine.wait(j) for j in ids]
 
-    # ---- warm-up (builds twiddle/coset tables, fills the memory pool)
-    for _ in range(max(args.warmup, 1)):
-        fri_ref = step_dev()
+    # ---- warm-up (builds twiddle/coset tables, fills the memory pool).  The engine's warm-up
+    # runs at least two rounds of its slots, so that the memory pool and the block cache hold
+    # what four jobs in flight use (growing the pool maps fresh device memory, which stalled
+    # jobs for up to a second on some boxes); the device path's warm-up steps come after it,
+    # directly before its timed region, so that they settle whatever blocks the engine's
+    # jobs took over.
+    fri_ref = step_dev()
     root_ref = root.copy()
-    # the engine's warm-up runs at least two rounds of its slots, so that the memory pool and
-    # the block cache hold what four jobs in flight use before the timed region (growing the
-    # pool maps fresh device memory, which stalled jobs for up to a second on some boxes)
     warm = run_engine(max(args.warmup, 2 * E2E_SLOTS))
     assert all((r[0] == root_ref).all() for r in warm), "engine root differs from the device path"
+    for _ in range(max(args.warmup, 1)):
+        fri_ref = step_dev()
 
     # ---- device-resident timed region (trace resident in HBM, > L2: no flush needed)
     sampler = ClockSampler(local_rank) if rank == 0 else None
@@ -494,16 +497,22 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         sampler.start()
         time.sleep(0.4)
     N.profile_start()
+    pool0 = N.pool_allocations()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
+    marks = []  # an event after every step: per-step device times (a stall shows as one long step)
     for _ in range(args.steps):
         last_pf = step_dev()
+        marks.append(torch.cuda.Event(enable_timing=True))
+        marks[-1].record(stream)
     ev1.record(stream)
     ev1.synchronize()
     barrier()
     kstats = N.profile_stop()
     clocks = sampler.stop() if sampler else None
     t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    pool_allocs = N.pool_allocations() - pool0
+    step_ms = sorted(a.elapsed_time(b) for a, b in zip([ev0] + marks[:-1], marks))
     assert (root == root_ref).all(), "root changed between steps"
     assert not with_fri or (last_pf.roots == fri_ref.roots).all(), "FRI commitments changed between steps"
     gpu_launches = sum(v[0] for v in kstats.values())
@@ -667,6 +676,13 @@ def run_ours(args, wl: dict, rank: int, world: int, local_rank: int) -> int:
         "gpu_launches": gpu_launches,
         "kernels": {k: {"launches": v[0], "ms_total": round(v[1], 3), "ms_max": round(v[2], 3)}
                     for k, v in sorted(kstats.items(), key=lambda kv: -kv[1][1])},
+        # per-step device time (min / median / max) and the part of a step no kernel of the
+        # library covered (host turnaround between launches and between steps)
+        "step_ms": {"min": round(step_ms[0], 3), "median": round(step_ms[len(step_ms) // 2], 3),
+                    "max": round(step_ms[-1], 3),
+                    "idle_per_step": round(1e3 * t_dev / args.steps - sum(v[1] for v in kstats.values()) / args.steps,
+                                           3),
+                    "pool_allocations": pool_allocs},
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)

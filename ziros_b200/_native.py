@@ -191,6 +191,7 @@ SIGNATURES = {
     "zkb_batch_profile": (_I, [_P, _P, _P, _P]),
     "zkb_debug_batch_stalled_run": (_I, [_P, _U64, _P]),
     "zkb_debug_device_allocations": (_U64, []),
+    "zkb_debug_pool_allocations": (_U64, []),
     "zkb_release_cached_memory": (_I, []),
     "zkb_engine_cancel": (_I, [_P, _U64]),
     "zkb_mmcs_verify_batch": (_I, [_P, _P, _P, _P, _SZ, _U64, _P, _P, _SZ]),
@@ -268,6 +269,11 @@ def inject_fault(kind: int, count: int = 1) -> None:
 def device_allocations() -> int:
     """Device allocations the library has made in this process (pool or cudaMalloc)."""
     return int(load().zkb_debug_device_allocations())
+
+
+def pool_allocations() -> int:
+    """Device allocations that missed the library's block cache (new memory from the pool)."""
+    return int(load().zkb_debug_pool_allocations())
 
 
 def release_cached_memory() -> None:

@@ -166,6 +166,7 @@ int zkb_debug_inject_fault(int kind, int count) {
 }
 
 uint64_t zkb_debug_device_allocations(void) { return device_alloc_count(); }
+uint64_t zkb_debug_pool_allocations(void) { return pool_alloc_count(); }
 
 int zkb_release_cached_memory(void) {
   clear_error();

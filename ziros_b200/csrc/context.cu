@@ -364,10 +364,12 @@ void set_thresholds(const zkb_thresholds &t) {
 
 namespace {
 std::atomic<uint64_t> g_device_allocs{0};
+std::atomic<uint64_t> g_pool_allocs{0};
 }
 
 void note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
 uint64_t device_alloc_count() { return g_device_allocs.load(std::memory_order_relaxed); }
+uint64_t pool_alloc_count() { return g_pool_allocs.load(std::memory_order_relaxed); }
 
 // ---- large blocks: an exact-size cache in front of the stream-ordered pool
 // Repeated jobs of one shape ask for the same sizes (staged trace, LDE, tree layers, FRI
@@ -445,6 +447,7 @@ int dev_alloc(void **p, size_t bytes, cudaStream_t s) {
       return ZKB_OK;
     }
   }
+  g_pool_allocs.fetch_add(1, std::memory_order_relaxed);
   cudaError_t e = cudaMallocAsync(p, rb, s);
   if (e == cudaErrorMemoryAllocation && cached) {
     cudaGetLastError();
