@@ -90,9 +90,9 @@ ZKB_API int zkb_debug_inject_fault(int kind, int count);
  * made in this process.  Tests read it around a call to check that the call allocated
  * nothing.  No counterpart in the reference. */
 ZKB_API uint64_t zkb_debug_device_allocations(void);
-/* Of those, the allocations that found no freed block of their size in the library's cache
- * and took new memory from the stream-ordered pool (which grows, mapping fresh memory,
- * when it has none free).  The bench reads it around its timed region.  No counterpart in
+/* Of those, the allocations of 1 MiB or more (the sizes the library caches) that found no
+ * freed block of their size in its cache and took new memory from the stream-ordered pool
+ * (which grows, mapping fresh memory, when it has none free).  The bench reads it around its timed region.  No counterpart in
  * the reference. */
 ZKB_API uint64_t zkb_debug_pool_allocations(void);
 /* Device memory the library keeps for reuse on the current device — freed blocks it caches

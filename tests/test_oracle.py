@@ -250,19 +250,3 @@ def test_fri_commit_oracle_relations(oracle):
                 i >>= 1
             assert (node == res["roots"][r]).all()
 
-
-def test_goldilocks_small_roots_are_powers_of_two(oracle):
-    """The Goldilocks register DIFs multiply by w_64^k as +-2^s (ntt_tile.cuh: gl_mul_pow2):
-    that needs w_64 = 2^39 for the field's two-adic generator (7^((p-1)/2^32))^(2^26), and
-    2^96 = -1.  The oracle's DFT of a 64-point unit vector gives the powers of w_64 itself."""
-    p = 2**64 - 2**32 + 1
-    w64 = pow(pow(7, (p - 1) >> 32, p), 2**26, p)
-    assert w64 == 2**39 and pow(2, 96, p) == p - 1
-    for k in range(64):
-        assert pow(w64, k, p) == pow(2, (39 * k) % 192, p)
-        assert pow(w64, -k % 64, p) == pow(2, (-39 * k) % 192, p)
-    import numpy as np
-    e1 = np.zeros((64, 1), dtype=np.uint64)
-    e1[1, 0] = 1
-    col = oracle.dft_batch(1, e1)[:, 0]
-    assert [int(v) for v in col] == [pow(2, (39 * f) % 192, p) for f in range(64)]

@@ -272,7 +272,7 @@ def device_allocations() -> int:
 
 
 def pool_allocations() -> int:
-    """Device allocations that missed the library's block cache (new memory from the pool)."""
+    """Device allocations of 1 MiB or more that missed the library's block cache (new pool memory)."""
     return int(load().zkb_debug_pool_allocations())
 
 

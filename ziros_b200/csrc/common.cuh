@@ -78,7 +78,8 @@ int dev_alloc(void **p, size_t bytes, cudaStream_t s);
 // zkb_debug_device_allocations() reads the count.
 void note_device_alloc();
 uint64_t device_alloc_count();
-// Allocations that missed the block cache (new memory from the stream-ordered pool).
+// Allocations of cached sizes (1 MiB or more) that missed the block cache and took new
+// memory from the stream-ordered pool.
 uint64_t pool_alloc_count();
 // Returns the cached blocks of the current device to the pool and trims the pool's unused
 // memory back to the device (for allocations outside the pool, e.g. a batch plan's arena).

@@ -447,7 +447,7 @@ int dev_alloc(void **p, size_t bytes, cudaStream_t s) {
       return ZKB_OK;
     }
   }
-  g_pool_allocs.fetch_add(1, std::memory_order_relaxed);
+  if (cached) g_pool_allocs.fetch_add(1, std::memory_order_relaxed);
   cudaError_t e = cudaMallocAsync(p, rb, s);
   if (e == cudaErrorMemoryAllocation && cached) {
     cudaGetLastError();

@@ -404,7 +404,6 @@ static SmallTw<F> small_twiddles(bool inverse) {
       st.q[e] = 0;
     acc = F::mul_host(acc, w);
   }
-  st.inverse = inverse ? 1u : 0u;
   return st;
 }
 

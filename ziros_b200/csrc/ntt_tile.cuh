@@ -38,13 +38,11 @@ struct PassGeom {
 
 // w_64^e, e < 32, for the register DIFs: BabyBear holds the canonical powers and their
 // Shoup quotients (products by these constants are Shoup products), Goldilocks the
-// canonical powers (q unused) — its register DIFs multiply by powers of two instead (below)
-// and only read the direction.
+// canonical powers (q unused).
 template <class F>
 struct SmallTw {
   typename F::T w[32];
   typename F::T q[32];
-  uint32_t inverse;  // 1: the table holds w_64^-e
 };
 
 // A twiddle staged in shared memory, in the form the kernels multiply by.  The cached
@@ -112,39 +110,6 @@ __device__ __forceinline__ uint64_t dif_mul<Goldilocks>(uint64_t a, uint64_t b, 
   return Goldilocks::mul(Goldilocks::sub(a, b), w);
 }
 
-// ---- Goldilocks: w_64 = 2^39 (mod p) for the field's two-adic generator, and 2^96 = -1, so
-// every power of w_64 is +-2^s with s < 96, and a product by one is shifts and the
-// special-form reduction — no multiplies.  E: the exponent of 2, 0 <= E < 192.
-__device__ __forceinline__ uint64_t gl_reduce128(uint64_t lo, uint64_t hi) {
-  // hi * 2^64 + lo with 2^64 = 2^32 - 1 and 2^96 = -1: lo - hi_hi + hi_lo * (2^32 - 1)
-  const uint64_t hi_hi = hi >> 32, hi_lo = hi & 0xFFFFFFFFull;
-  uint64_t t0 = lo - hi_hi;
-  if (lo < hi_hi) t0 -= Goldilocks::EPS;  // + p; the raw difference is above EPS then
-  const uint64_t t1 = (hi_lo << 32) - hi_lo;
-  uint64_t r = t0 + t1;
-  if (r < t1) r += Goldilocks::EPS;  // 2^64 = EPS; no second carry
-  return Goldilocks::canon(r);
-}
-
-template <int E>
-__device__ __forceinline__ uint64_t gl_mul_pow2(uint64_t x) {
-  static_assert(E >= 0 && E < 192, "exponent of 2 out of range");
-  constexpr int S = E % 96;
-  uint64_t y;
-  if constexpr (S == 0) {
-    y = x;
-  } else if constexpr (S < 64) {
-    y = gl_reduce128(x << S, x >> (64 - S));
-  } else {
-    // x * 2^S = m * 2^64 + top * 2^128 with m = low 64 bits of x << (S - 64), top < 2^32;
-    // 2^128 = -2^32, and top * 2^32 < p
-    const uint64_t m = x << (S - 64), top = x >> (128 - S);
-    y = Goldilocks::sub(gl_reduce128(0, m), top << 32);
-  }
-  if constexpr (E >= 96) y = Goldilocks::neg(y);
-  return y;
-}
-
 // Compile-time loop: fn(std::integral_constant<int, I>) for I = 0..N-1, so every index
 // derived from I (bit reversals, twiddle slots) is a constant expression.
 template <class Fn, int... I>
@@ -156,39 +121,10 @@ __device__ __forceinline__ void sfor(Fn &&fn) {
   if constexpr (N > 0) sfor_impl(fn, std::make_integer_sequence<int, N>{});
 }
 
-// Goldilocks register DIF with its twiddles as powers of two (w_64^k = 2^(39k mod 192); the
-// inverse direction's w_64^-k = 2^(-39k mod 192)), chosen at compile time.
-template <int LR, bool INV>
-__device__ __forceinline__ void dif_reg_gl(uint64_t (&x)[1 << LR]) {
-  sfor<LR>([&](auto sc) {
-    constexpr int s = LR - 1 - decltype(sc)::value;
-    constexpr int h = 1 << s;
-    sfor<(1 << LR) / 2>([&](auto bc) {
-      constexpr int b = decltype(bc)::value;
-      constexpr int j = b % h, g = (b / h) * 2 * h;
-      constexpr int k = j << (5 - s);
-      constexpr int E = INV ? (192 - (39 * k) % 192) % 192 : (39 * k) % 192;
-      const uint64_t a = x[g + j], c = x[g + j + h];
-      x[g + j] = Goldilocks::add(a, c);
-      if constexpr (j == 0)
-        x[g + j + h] = Goldilocks::sub(a, c);
-      else
-        x[g + j + h] = gl_mul_pow2<E>(Goldilocks::sub(a, c));
-    });
-  });
-}
-
 // In-register radix-2 DIF of 2^LR points: natural in, x[t] = X[rev(t)] out.
 template <class F, int LR>
 __device__ __forceinline__ void dif_reg(typename F::T (&x)[1 << LR], const SmallTw<F> &st) {
   using T = typename F::T;
-  if constexpr (std::is_same<F, Goldilocks>::value) {
-    if (st.inverse)
-      dif_reg_gl<LR, true>(x);
-    else
-      dif_reg_gl<LR, false>(x);
-    return;
-  }
   sfor<LR>([&](auto sc) {
     constexpr int s = LR - 1 - decltype(sc)::value;
     constexpr int h = 1 << s;
