@@ -558,8 +558,11 @@ ZKB_API int zkb_batch_run(zkb_batch *batch, void *stream);
  * row-major, canonical elements; pinned host memory for the copies to run asynchronously).
  * The copies overlap the commitment: a copy stream takes the traces in groups (about 1/64
  * of the batch's cells each, small traces first and last, the largest in the middle), and
- * each group's LDEs and trees — one graph per group, captured at creation — run on `stream`
- * as soon as the group's copies have landed.  A persistent plan copies every trace first,
+ * each group's LDEs and trees — one graph per group, captured at the plan's first host run
+ * (which also allocates the second lane below) — run as soon as
+ * the group's copies have landed, the groups alternating between `stream` and a second
+ * stream of the plan (with a second coefficient-scratch set, when it takes at most 1/8 of
+ * free device memory); `stream` waits for all of it.  A persistent plan copies every trace first,
  * then runs its kernel.  Pinned sources are read until
  * `stream` has passed the run; pageable ones are staged before the call returns.  Roots
  * and trees as after zkb_batch_run.  No counterpart in the reference. */

@@ -64,6 +64,7 @@ struct JobTables {
 struct HostGroup {
   std::vector<int> traces;
   std::vector<char> member;  // per batch index
+  int lane = 0;              // 0: the caller's stream and the plan's scratch, 1: the second lane
   JobTables jobs;
   cudaEvent_t copied = nullptr;
   cudaGraph_t graph = nullptr;
@@ -174,6 +175,14 @@ struct zkb_batch {
   cudaStream_t s_copy = nullptr;
   cudaEvent_t ev_host = nullptr, ev_copied = nullptr;
   std::vector<HostGroup> host_groups;
+  // a second lane for the host groups: its own stream and a second coefficient-scratch set,
+  // so that a group's LDEs overlap the tail of the group before it (graph plans only)
+  uint32_t host_lanes = 1;
+  bool host_ready = false;  // lanes set up and group graphs captured (at the first run_host)
+  cudaStream_t s_lane = nullptr;
+  cudaEvent_t ev_lane = nullptr;
+  void *d_coef2_base = nullptr;
+  std::vector<void *> d_coef2;
   P2Params<BabyBear, 16> p_bb16;
   P2Params<Goldilocks, 16> p_gl16;
   P2Params<Goldilocks, 12> p_gl12;
@@ -196,6 +205,9 @@ struct zkb_batch {
     }
     if (ev_host) cudaEventDestroy(ev_host);
     if (ev_copied) cudaEventDestroy(ev_copied);
+    if (ev_lane) cudaEventDestroy(ev_lane);
+    if (s_lane) cudaStreamDestroy(s_lane);
+    if (d_coef2_base) cudaFree(d_coef2_base);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (s_copy) cudaStreamDestroy(s_copy);
     for (auto s : s_br) cudaStreamDestroy(s);
@@ -206,15 +218,16 @@ struct zkb_batch {
   uint64_t rows_of(size_t i) const { return 1ull << (shapes[i].log_h + log_b); }
 
   // ---- launches of one run, enqueued on `origin` (captured or direct)
-  int lde_one(size_t i, cudaStream_t s, const LdeTune *t) {
+  int lde_one(size_t i, cudaStream_t s, const LdeTune *t, int lane = 0) {
     const int lh = (int)shapes[i].log_h;
     const uint32_t w = shapes[i].width;
     const int br = branch_of(i);
+    void *scratch = lane ? d_coef2[br] : d_coef[br];
     if (spec.field == FIELD_BABYBEAR)
       return ntt_lde_dev<BabyBear>((const uint32_t *)d_in[i], lh, w, (int)log_b, BabyBear::GENERATOR, true,
-                                   (uint32_t *)d_lde[i], s, t, (uint32_t *)d_coef[br]);
+                                   (uint32_t *)d_lde[i], s, t, (uint32_t *)scratch);
     return ntt_lde_dev<Goldilocks>((const uint64_t *)d_in[i], lh, w, (int)log_b, Goldilocks::GENERATOR, true,
-                                   (uint64_t *)d_lde[i], s, t, (uint64_t *)d_coef[br]);
+                                   (uint64_t *)d_lde[i], s, t, (uint64_t *)scratch);
   }
   int branch_of(size_t i) const {
     for (size_t b = 0; b < branch_traces.size(); b++)
@@ -240,8 +253,9 @@ struct zkb_batch {
   int hash_dispatch(unsigned threads, cudaStream_t s) { return hash_tables(joint, threads, s); }
 
   // The LDEs of the `member` traces (every trace when NULL), forked over their branches
-  // (each branch in its own order, with its own coefficient scratch) and joined on origin.
-  int enqueue_ldes(const std::vector<char> *member, cudaStream_t origin) {
+  // (each branch in its own order, with its own coefficient scratch of the lane's set) and
+  // joined on origin.
+  int enqueue_ldes(const std::vector<char> *member, cudaStream_t origin, int lane = 0) {
     const uint32_t nb = (uint32_t)branch_traces.size();
     ZKB_CHECK_CUDA(cudaEventRecord(ev_fork, origin));
     for (uint32_t b = 0; b < nb; b++) {
@@ -250,7 +264,7 @@ struct zkb_batch {
       if (!any) continue;
       ZKB_CHECK_CUDA(cudaStreamWaitEvent(s_br[b], ev_fork, 0));
       for (int i : branch_traces[b])
-        if (!member || (*member)[i]) ZKB_TRY(lde_one((size_t)i, s_br[b], &tune[i]));
+        if (!member || (*member)[i]) ZKB_TRY(lde_one((size_t)i, s_br[b], &tune[i], lane));
       ZKB_CHECK_CUDA(cudaEventRecord(ev_br[b], s_br[b]));
       ZKB_CHECK_CUDA(cudaStreamWaitEvent(origin, ev_br[b], 0));
     }
@@ -258,8 +272,41 @@ struct zkb_batch {
   }
 
   int enqueue_group(const HostGroup &g, cudaStream_t origin) {
-    ZKB_TRY(enqueue_ldes(&g.member, origin));
+    ZKB_TRY(enqueue_ldes(&g.member, origin, g.lane));
     return hash_tables(g.jobs, leaf_threads, origin);
+  }
+
+  // A second coefficient-scratch set (each branch's largest trace again) when it takes at
+  // most an eighth of free device memory: the host groups then alternate between two lanes.
+  int setup_host_lanes() {
+    host_lanes = 1;
+    if (host_groups.size() < 2) return ZKB_OK;
+    std::vector<uint64_t> need(branch_traces.size(), 0);
+    uint64_t total = 0;
+    for (size_t b = 0; b < branch_traces.size(); b++) {
+      for (int i : branch_traces[b]) need[b] = std::max<uint64_t>(need[b], (1ull << shapes[i].log_h) * shapes[i].width * es);
+      need[b] = align256(std::max<uint64_t>(need[b], 256));
+      total += need[b];
+    }
+    size_t free_b = 0, total_b = 0;
+    ZKB_CHECK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (total > free_b / 8) {
+      for (auto &g : host_groups) g.lane = 0;
+      return ZKB_OK;
+    }
+    note_device_alloc();
+    ZKB_CHECK_CUDA(cudaMalloc(&d_coef2_base, total));
+    d_coef2.assign(branch_traces.size(), nullptr);
+    uint64_t o = 0;
+    for (size_t b = 0; b < branch_traces.size(); b++) {
+      d_coef2[b] = (char *)d_coef2_base + o;
+      o += need[b];
+    }
+    ZKB_CHECK_CUDA(cudaStreamCreateWithFlags(&s_lane, cudaStreamNonBlocking));
+    ZKB_CHECK_CUDA(cudaEventCreateWithFlags(&ev_lane, cudaEventDisableTiming));
+    for (size_t k = 0; k < host_groups.size(); k++) host_groups[k].lane = (int)(k % 2);
+    host_lanes = 2;
+    return ZKB_OK;
   }
 
   // One graph per host group (the group's launches captured on s_main).
@@ -292,8 +339,10 @@ struct zkb_batch {
 
   // A run whose traces come from host memory, the copies overlapped with the commitment:
   // the copy stream takes the traces in groups (about 1/64 of the batch's cells each, a
-  // larger trace by itself), and each group's LDEs and trees run on origin as soon as its
-  // last copy has landed, while the next groups copy.  This is a two-stage flow (copy, then
+  // larger trace by itself), and each group's LDEs and trees run as soon as its last copy
+  // has landed, while the next groups copy — the groups alternating between origin and a
+  // second lane with its own scratch (when memory allows), so that a group's LDEs overlap
+  // the small top levels of the trees of the group before it.  This is a two-stage flow (copy, then
   // compute) whose two stages run at similar rates per cell (the compute a little slower
   // or faster, depending on the host link): the work done outside the overlap is the
   // first group's copy and the last group's compute, so the copy order puts small traces
@@ -306,8 +355,18 @@ struct zkb_batch {
   int run_host(const void *const *src, cudaStream_t origin) {
     const size_t n = shapes.size();
     for (size_t i = 0; i < n; i++) ZKB_REQUIRE(src[i] != nullptr, "trace %zu: null host source", i);
+    if (!persistent && !host_ready) {
+      // set up at the first host run, so that plans never run from host memory keep the
+      // memory and the creation time
+      if (use_graph) {
+        ZKB_TRY(setup_host_lanes());
+        ZKB_TRY(capture_groups());
+      }
+      host_ready = true;
+    }
     ZKB_CHECK_CUDA(cudaEventRecord(ev_host, origin));
     ZKB_CHECK_CUDA(cudaStreamWaitEvent(s_copy, ev_host, 0));
+    if (host_lanes == 2) ZKB_CHECK_CUDA(cudaStreamWaitEvent(s_lane, ev_host, 0));
     int rc = ZKB_OK;
     if (persistent) {
       for (size_t i = 0; i < n && rc == ZKB_OK; i++) rc = copy_host(i, src[i], s_copy);
@@ -316,22 +375,28 @@ struct zkb_batch {
         HostGroup &g = host_groups[k];
         for (size_t q = 0; q < g.traces.size() && rc == ZKB_OK; q++) rc = copy_host(g.traces[q], src[g.traces[q]], s_copy);
         if (rc != ZKB_OK) break;
-        if (cudaEventRecord(g.copied, s_copy) != cudaSuccess || cudaStreamWaitEvent(origin, g.copied, 0) != cudaSuccess) {
+        cudaStream_t ls = g.lane ? s_lane : origin;
+        if (cudaEventRecord(g.copied, s_copy) != cudaSuccess || cudaStreamWaitEvent(ls, g.copied, 0) != cudaSuccess) {
           set_error("copy ordering failed: %s", cudaGetErrorString(cudaGetLastError()));
           rc = ZKB_ERR_CUDA;
           break;
         }
         if (g.exec) {
-          if (cudaGraphLaunch(g.exec, origin) != cudaSuccess) {
+          if (cudaGraphLaunch(g.exec, ls) != cudaSuccess) {
             set_error("group graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
             rc = ZKB_ERR_CUDA;
           }
         } else {
-          rc = enqueue_group(g, origin);
+          rc = enqueue_group(g, ls);
         }
       }
     }
-    // origin joins the copy stream, also after an error (the sources are read until then)
+    // origin joins the second lane and the copy stream, also after an error (the sources are
+    // read until then)
+    if (host_lanes == 2) {
+      ZKB_CHECK_CUDA(cudaEventRecord(ev_lane, s_lane));
+      ZKB_CHECK_CUDA(cudaStreamWaitEvent(origin, ev_lane, 0));
+    }
     ZKB_CHECK_CUDA(cudaEventRecord(ev_copied, s_copy));
     ZKB_CHECK_CUDA(cudaStreamWaitEvent(origin, ev_copied, 0));
     ZKB_TRY(rc);
@@ -913,7 +978,7 @@ int batch_build(zkb_batch *b, const zkb_batch_options &opt) {
   ZKB_TRY(rc);
   if (opt.autotune) cache.save();
   if (b->use_graph) ZKB_TRY(b->capture());
-  if (b->use_graph && !b->persistent) ZKB_TRY(b->capture_groups());
+
 
   // ---- borrowed per-trace trees for openings
   for (size_t i = 0; i < n; i++) {
