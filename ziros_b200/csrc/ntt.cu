@@ -347,6 +347,19 @@ static int pass_tensor_map(CUtensorMap *m, const void *base, size_t es, const Pa
   return ZKB_OK;
 }
 
+// Whether the tiles of a K-bit pass at bits [lo, lo + K) of `n_blocks` transforms of 2^L
+// rows can come by tensor copy: the mode is on, C columns and the row stride are multiples of
+// 16 bytes, the base is 16-byte aligned, and the tensor map's limits hold (strides below
+// 2^40 bytes, dimensions up to 2^32).  Otherwise the tile keeps its register loads.
+static bool tma_tiles(const void *base, size_t es, uint32_t width, uint32_t C, int L, int lo, int K, uint64_t n_blocks,
+                      uint32_t cols) {
+  if (!cols || ntt_tile_loads().load() != 1 || C * es < 16 || (width * es) % 16 != 0 || ((uintptr_t)base & 15) != 0)
+    return false;
+  const uint64_t row = (uint64_t)width * es;
+  if (L - lo - K < 0 || lo + K > 40 || (row << (lo + K)) >= (1ull << 40) || (row >> (40 - lo - K)) != 0) return false;
+  return ((1ull << (L - lo - K)) * n_blocks) <= (1ull << 32);
+}
+
 template <class F, int LR1, int LR2, int C>
 static int launch_pass_tma_c(const typename F::T *src, typename F::T *out, const PassGeom &g, uint32_t cols,
                              uint64_t n_blocks, uint64_t ctas, const typename F::T *tw, typename F::T scale,
@@ -425,12 +438,10 @@ static int launch_pass(const typename F::T *src, typename F::T *out, const PassG
                        const typename F::T *tw, typename F::T scale, const SmallTw<F> &st,
                        uint32_t C, cudaStream_t s, uint32_t cols = 0, uint64_t n_blocks = 0) {
   // tensor-copy tile loads where every copy's start and the row stride are 16-byte aligned
-  constexpr size_t es = sizeof(typename F::T);
-  if (cols && ntt_tile_loads().load() == 1 && C * es >= 16 && (g.width * es) % 16 == 0 &&
-      ((uintptr_t)src & 15) == 0) {
+  if (tma_tiles(src, sizeof(typename F::T), g.width, C, g.L, g.lo, LR1 + LR2, n_blocks, cols)) {
     switch (C) {
       case 16:
-        if constexpr (es == 4) return launch_pass_tma_c<F, LR1, LR2, 16>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
+        if constexpr (sizeof(typename F::T) == 4) return launch_pass_tma_c<F, LR1, LR2, 16>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
         break;
       case 8: return launch_pass_tma_c<F, LR1, LR2, 8>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
       case 4: return launch_pass_tma_c<F, LR1, LR2, 4>(src, out, g, cols, n_blocks, ctas, tw, scale, st, s);
@@ -582,8 +593,7 @@ static int launch_fused_c(const typename F::T *in, typename F::T *out, const Fus
   using T = typename F::T;
   constexpr unsigned threads = C << LR2;
   const uint64_t ctas0 = (uint64_t)g.chunks_per_row * g.blocks;
-  if (cols && ntt_tile_loads().load() == 1 && C * sizeof(T) >= 16 && (g.width * sizeof(T)) % 16 == 0 &&
-      ((uintptr_t)in & 15) == 0) {
+  if (tma_tiles(in, sizeof(T), g.width, C, g.L, 0, LR1 + LR2, 1, cols)) {
     // block B's rows as the tile of a pass at bits [0, K) of one transform
     PassGeom pg;
     pg.L = g.L;
