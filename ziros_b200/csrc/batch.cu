@@ -295,7 +295,12 @@ struct zkb_batch {
       return ZKB_OK;
     }
     note_device_alloc();
-    ZKB_CHECK_CUDA(cudaMalloc(&d_coef2_base, total));
+    if (cudaMalloc(&d_coef2_base, total) != cudaSuccess) {  // one lane, then
+      cudaGetLastError();
+      d_coef2_base = nullptr;
+      for (auto &g : host_groups) g.lane = 0;
+      return ZKB_OK;
+    }
     d_coef2.assign(branch_traces.size(), nullptr);
     uint64_t o = 0;
     for (size_t b = 0; b < branch_traces.size(); b++) {
