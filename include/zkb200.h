@@ -178,7 +178,7 @@ ZKB_API int zkb_dft_batch_noalloc_dev(int field, void *d_rowmajor, uint32_t log_
                                       int inverse, void *stream);
 
 /* Tile loads of the NTT passes and the fused LDE middle (DFT, LDE, commits;
- * process-wide): 1 = one tensor copy (TMA, cp.async.bulk.tensor, no multicast) of each
+ * process-wide): 1 = one tensor copy (TMA, cp.async.bulk.tensor into the CTA's own shared memory) of each
  * tile into shared memory (the default), used where the row stride and the column chunk
  * are multiples of 16 bytes (BabyBear: width a multiple of 4, chunks of 4 columns or more;
  * Goldilocks: even width, chunks of 4 or 8; other tiles keep the loads); 0 = coalesced

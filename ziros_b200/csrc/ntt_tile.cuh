@@ -143,7 +143,7 @@ __device__ __forceinline__ void dif_reg(typename F::T (&x)[1 << LR], const Small
 
 // ---- tensor-copy (TMA) tile loads
 // A pass tile can arrive in shared memory as ONE tensor copy (cp.async.bulk.tensor,
-// no multicast, this GPU's memory only) instead of R1 coalesced loads per thread: the
+// one CTA's destination, this GPU's memory only) instead of R1 coalesced loads per thread: the
 // tensor map views a column segment as 5 dimensions (column, row bits below the pass,
 // the pass's bits in two parts of at most 8, the bits above it with the transform index)
 // and the box is C columns x 2^K rows, so row r of the tile lands at r * C.  Completion is
