@@ -419,10 +419,17 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
   auto tree = std::make_unique<zkb_tree>();
   tree->t.stream = s;
   ZKB_CHECK_CUDA(cudaGetDevice(&tree->t.device));
+  // A host trace of at least two 64-column slabs (BabyBear, width-16 hasher) is uploaded a
+  // slab at a time, and each slab's LDE and leaf absorption start once it has landed, while
+  // the next slab crosses the link (see the leaf fill below).
+  constexpr uint32_t kSlab = 64;
+  const bool slabbed = h_trace && spec.field == FIELD_BABYBEAR && spec.width == 16 && width >= 2 * kSlab && log_h >= 1;
   ScratchBuf staged;
   if (h_trace) {
     ZKB_TRY(staged.alloc(n * width * es, s));
-    if (upload_mu) {
+    if (slabbed) {
+      // uploaded below, slab by slab
+    } else if (upload_mu) {
       // one upload at a time: concurrent jobs would split the PCIe link and all start
       // computing late; serialised, each upload runs under the other jobs' kernels.  The
       // link is taken per 256 MiB piece, the upload with the fewest bytes left first, so a
@@ -448,18 +455,22 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
     }
     d_trace = staged.p;
   }
-  if (stages) stages->uploaded = std::chrono::steady_clock::now();
-  // an engine job waits here, its trace on the device, until the jobs of its size class
-  // ahead of it have finished computing
-  if (compute_lock) compute_lock->lock();
-  if (stages) stages->lock_taken = std::chrono::steady_clock::now();
+  if (!slabbed) {
+    if (stages) stages->uploaded = std::chrono::steady_clock::now();
+    // an engine job waits here, its trace on the device, until the jobs of its size class
+    // ahead of it have finished computing
+    if (compute_lock) compute_lock->lock();
+    if (stages) stages->lock_taken = std::chrono::steady_clock::now();
+  }
   void *lde = nullptr;
   ZKB_TRY(dev_alloc(&lde, N * width * es, s));
   tree->t.owned.push_back(lde);
   // A staged copy of a host trace is ours: the inverse passes run in place on it
   // instead of in a separate coefficient scratch.
-  int rc;
-  if (spec.field == FIELD_BABYBEAR)
+  int rc = ZKB_OK;
+  if (slabbed)
+    ;  // slab by slab in the leaf fill
+  else if (spec.field == FIELD_BABYBEAR)
     rc = ntt_lde_dev<BabyBear>((const uint32_t *)d_trace, (int)log_h, width, (int)log_blowup,
                                BabyBear::GENERATOR, true, (uint32_t *)lde, s, nullptr,
                                h_trace ? staged.as<uint32_t>() : nullptr);
@@ -485,7 +496,80 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
   if (fused_reduction) {
     ZKB_REQUIRE(alpha != nullptr, "null alpha");
     ZKB_TRY(alpha_powers_dev(alpha, width, &apow, s));
-    const LeafCombine comb{apow.as<uint4>(), (uint4 *)cw};
+  }
+  const LeafCombine comb{fused_reduction ? apow.as<uint4>() : nullptr, (uint4 *)cw};
+  if (slabbed) {
+    // Slab k (columns [64k, 64k + 64)) crosses the link on a copy stream of its own, in
+    // pieces of at most 256 MiB through the engine's upload gate; once it has landed, its
+    // LDE (inverse passes in place on the staged columns, row stride `width`) and the leaf
+    // sponge over its columns (state carried between slabs, the alpha-reduction summed)
+    // are enqueued on s, so they run while the next slab is copied.  An engine job takes
+    // its size class's compute lock before its first slab's kernels if the lock is free,
+    // else uploads every slab first and then waits for it, as an unslabbed job does.
+    ScratchBuf carry;
+    ZKB_TRY(carry.alloc(N * 16 * sizeof(uint32_t), s));
+    struct StreamHolder {
+      cudaStream_t c = nullptr;
+      ~StreamHolder() {
+        if (c) cudaStreamDestroy(c);
+      }
+    } cs;
+    ZKB_CHECK_CUDA(cudaStreamCreateWithFlags(&cs.c, cudaStreamNonBlocking));
+    const uint32_t nslabs = (width + kSlab - 1) / kSlab;
+    const LeafFill fill = [&](void *digests) -> int {
+      uint32_t copied = 0, done = 0;
+      bool locked = compute_lock == nullptr;
+      auto compute = [&]() -> int {
+        for (; done < copied; done++) {
+          const uint32_t c0 = done * kSlab, nc = std::min(kSlab, width - c0);
+          ZKB_TRY(ntt_lde_dev<BabyBear>(staged.as<uint32_t>() + c0, (int)log_h, nc, (int)log_blowup,
+                                        BabyBear::GENERATOR, true, (uint32_t *)lde + c0, s, nullptr,
+                                        staged.as<uint32_t>() + c0, width));
+          ZKB_TRY(hash_rows_slab_dev(spec, (const uint32_t *)lde, width, c0, nc, N, carry.as<uint32_t>(), done == 0,
+                                     done + 1 == nslabs, (uint32_t *)digests, fused_reduction ? &comb : nullptr, s));
+        }
+        return ZKB_OK;
+      };
+      const uint64_t total = n * width * es;
+      uint64_t sent = 0;
+      const uint64_t ticket = upload_mu ? upload_mu->ticket() : 0;
+      for (uint32_t k = 0; k < nslabs; k++) {
+        const uint32_t c0 = k * kSlab, nc = std::min(kSlab, width - c0);
+        const uint64_t row_bytes = (uint64_t)nc * es;
+        const uint64_t rows_per_piece = std::max<uint64_t>(1, (256ull << 20) / row_bytes);
+        for (uint64_t r0 = 0; r0 < n; r0 += rows_per_piece) {
+          const uint64_t rows = std::min<uint64_t>(rows_per_piece, n - r0);
+          if (upload_mu) upload_mu->acquire(total - sent, ticket);
+          const size_t off = (size_t)(r0 * width + c0) * es;
+          int prc = ZKB_OK;
+          const cudaError_t e = cudaMemcpy2DAsync((char *)staged.p + off, (size_t)width * es,
+                                                  (const char *)h_trace + off, (size_t)width * es, row_bytes, rows,
+                                                  cudaMemcpyHostToDevice, cs.c);
+          if (e != cudaSuccess) {
+            set_error("cudaMemcpy2DAsync of a trace slab failed: %s", cudaGetErrorString(e));
+            prc = ZKB_ERR_CUDA;
+          }
+          if (prc == ZKB_OK) prc = wait_stream(cs.c);
+          if (upload_mu) upload_mu->release();
+          ZKB_TRY(prc);
+          sent += rows * row_bytes;
+        }
+        copied++;
+        if (!locked && compute_lock->try_lock()) {
+          locked = true;
+          if (stages) stages->lock_taken = std::chrono::steady_clock::now();
+        }
+        if (locked) ZKB_TRY(compute());
+      }
+      if (stages) stages->uploaded = std::chrono::steady_clock::now();
+      if (!locked) {
+        compute_lock->lock();
+        if (stages) stages->lock_taken = std::chrono::steady_clock::now();
+      }
+      return compute();
+    };
+    ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s, false, nullptr, &fill));
+  } else if (fused_reduction) {
     ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s, false, &comb));
   } else {
     ZKB_TRY(mmcs_build_dev(spec, mats, &tree->t, s));

@@ -4,6 +4,7 @@
 #include <map>
 #include <array>
 #include <condition_variable>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <set>
@@ -38,11 +39,13 @@ struct LdeTune {
 };
 int lde_tune_check(int field, uint32_t width, const LdeTune &t);
 // p3 coset_lde_batch (+ bit_reverse_rows when bitrev): d_out holds 2^(log_h+log_b) rows.
-// coef_scratch (2^log_h x width), when given, is used instead of an allocation.
+// coef_scratch (2^log_h x width), when given, is used instead of an allocation.  stride
+// (0: width) is the row stride of d_trace, d_out and coef_scratch when the LDE covers
+// `width` columns of wider matrices (bitrev only).
 template <class F>
 int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log_b,
                 typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s,
-                const LdeTune *tune = nullptr, typename F::T *coef_scratch = nullptr);
+                const LdeTune *tune = nullptr, typename F::T *coef_scratch = nullptr, uint32_t stride = 0);
 // Natural-order DFT with caller-supplied twiddle (2^log_h) and temp (2^log_h x width) buffers.
 template <class F>
 int ntt_dft_into(typename F::T *d, int log_h, uint32_t width, bool inverse, typename F::T *tw_buf,
@@ -81,8 +84,17 @@ struct LeafCombine {
   const uint4 *apow;
   uint4 *out;
 };
+// Writes a tree's layer 0 (the leaf digests) in place of the leaf-hash launch.
+using LeafFill = std::function<int(void *digests)>;
 int mmcs_build_dev(const HasherSpec &h, const std::vector<TreeMatrix> &mats, DeviceTree *tree,
-                   cudaStream_t s, bool fri_layer = false, const LeafCombine *comb = nullptr);
+                   cudaStream_t s, bool fri_layer = false, const LeafCombine *comb = nullptr,
+                   const LeafFill *fill = nullptr);
+// Leaf sponge over columns [c0, c0 + ncols) of a BabyBear matrix (width-16 hasher) arriving
+// a slab at a time: state carried in `carry` (16 words per row) between slabs, digests on
+// the last; with comb, the slab's alpha-reduction written (first) or added to comb->out.
+int hash_rows_slab_dev(const HasherSpec &h, const uint32_t *mat, uint64_t stride, uint64_t c0, uint64_t ncols,
+                       uint64_t height, uint32_t *carry, bool first, bool last, uint32_t *digests,
+                       const LeafCombine *comb, cudaStream_t s);
 // alpha^j * 2^64 mod p per coefficient, j < width, uploaded (uint4 per column).
 int alpha_powers_dev(const uint32_t alpha[4], uint32_t width, ScratchBuf *out, cudaStream_t s);
 // Copy the root (spec.out elements) to host memory (synchronises the stream).

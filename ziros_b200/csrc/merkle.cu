@@ -124,6 +124,83 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// The same sponge over columns [c0, c0 + ncols) of the rows only (row stride `stride`), for a
+// matrix that arrives a slab of columns at a time: the sponge state comes from `carry`
+// (16 words per row, internal domain; none on the first slab) and goes back there, or on
+// the last slab the digest goes to `digests`.  c0 is a multiple of 8 (slabs hold whole
+// absorbed chunks; only the last slab may end in a partial one), so the chunks and
+// permutations are exactly the full row's.  With apow, the rows' alpha-reduction over
+// these columns is written (first slab) or added (mod p) to comb: the sum of the slabs'
+// reductions is the whole row's.
+__global__ void __launch_bounds__(128)
+    hash_rows_slab_kernel(const uint32_t *__restrict__ mat, uint64_t stride, uint64_t c0, uint64_t ncols,
+                          uint64_t height, uint32_t *__restrict__ carry, int first, int last,
+                          uint32_t *__restrict__ digests, const __grid_constant__ P2Params<BabyBear, 16> p,
+                          const uint4 *__restrict__ apow, uint4 *__restrict__ comb) {
+  using D = Dom<BabyBear>;
+  using B = BabyBear;
+  for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < height;
+       row += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t s[16];
+    if (first) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) s[i] = 0;
+    } else {
+      const uint4 *cp = reinterpret_cast<const uint4 *>(carry + row * 16);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint4 v = cp[q];
+        s[4 * q] = v.x;
+        s[4 * q + 1] = v.y;
+        s[4 * q + 2] = v.z;
+        s[4 * q + 3] = v.w;
+      }
+    }
+    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    const uint32_t *rp = mat + row * stride + c0;
+    const uint4 *ap = apow ? apow + c0 : nullptr;
+    for (uint64_t c = 0; c < ncols; c += 8) {
+#pragma unroll
+      for (int i = 0; i < 8; i += 2) {
+        if (c + i < ncols) {
+          const uint32_t v0 = rp[c + i];
+          s[i] = D::enter(v0);
+          uint32_t v1 = 0;
+          if (c + i + 1 < ncols) {
+            v1 = rp[c + i + 1];
+            s[i + 1] = D::enter(v1);
+          }
+          if (ap) {
+            const uint4 w0 = ap[c + i];
+            const uint4 w1 = c + i + 1 < ncols ? ap[c + i + 1] : make_uint4(0, 0, 0, 0);
+            a0 += B::mont_lazy_sum(v0, w0.x, v1, w1.x);
+            a1 += B::mont_lazy_sum(v0, w0.y, v1, w1.y);
+            a2 += B::mont_lazy_sum(v0, w0.z, v1, w1.z);
+            a3 += B::mont_lazy_sum(v0, w0.w, v1, w1.w);
+          }
+        }
+      }
+      p2_permute<BabyBear, 16>(s, p);
+    }
+    if (last) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) digests[row * 8 + i] = D::leave(s[i]);
+    } else {
+      uint4 *cp = reinterpret_cast<uint4 *>(carry + row * 16);
+#pragma unroll
+      for (int q = 0; q < 4; q++) cp[q] = make_uint4(s[4 * q], s[4 * q + 1], s[4 * q + 2], s[4 * q + 3]);
+    }
+    if (ap) {
+      uint4 r = make_uint4(B::mont_reduce(a0), B::mont_reduce(a1), B::mont_reduce(a2), B::mont_reduce(a3));
+      if (!first) {
+        const uint4 o = comb[row];
+        r = make_uint4(B::add(o.x, r.x), B::add(o.y, r.y), B::add(o.z, r.z), B::add(o.w, r.w));
+      }
+      comb[row] = r;
+    }
+  }
+}
+
 // next[i] = compress(prev[2i], prev[2i+1]); with `inj` (digests of the rows injected at
 // this layer, inj_h of them) next[i] = compress(that, i < inj_h ? inj[i] : 0).
 template <class F, int W>
@@ -176,7 +253,8 @@ static int log2_ceil(uint64_t x) {
 
 template <class F, int W>
 static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &mats,
-                           DeviceTree *t, cudaStream_t s, bool fri_layer, const LeafCombine *comb) {
+                           DeviceTree *t, cudaStream_t s, bool fri_layer, const LeafCombine *comb,
+                           const LeafFill *fill) {
   const char *leaf_name = fri_layer ? "fri_leaf_hash" : "merkle_leaf_hash";
   const char *comp_name = fri_layer ? "fri_compress" : "merkle_compress";
   using T = typename F::T;
@@ -254,7 +332,11 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
   // jobs higher stream priority) get SMs in between instead of waiting for the whole grid.
   const unsigned cap = 1u << 30;
   (void)ctx;
-  if constexpr (std::is_same<F, BabyBear>::value && W == 16) {
+  if (fill) {
+    // the caller writes layer 0 (e.g. slab by slab as the matrix arrives)
+    ZKB_REQUIRE(nm == 1 && comb == nullptr, "internal: leaves written by the caller take one matrix");
+    ZKB_TRY((*fill)(layers));
+  } else if constexpr (std::is_same<F, BabyBear>::value && W == 16) {
     if (comb) {
       ZKB_REQUIRE(nm == 1, "the fused alpha-reduction takes one matrix");
       ZKB_LAUNCH(leaf_name, s, hash_rows_combine_kernel<<<grid_for(max_h, thr, cap), thr, 0, s>>>((const uint32_t *)ml.ptr[0], ml.width[0], max_h, layers, p, comb->apow, comb->out));
@@ -296,13 +378,28 @@ static int build_tree_impl(const HasherSpec &h, const std::vector<TreeMatrix> &m
 }
 
 int mmcs_build_dev(const HasherSpec &h, const std::vector<TreeMatrix> &mats, DeviceTree *tree,
-                   cudaStream_t s, bool fri_layer, const LeafCombine *comb) {
+                   cudaStream_t s, bool fri_layer, const LeafCombine *comb, const LeafFill *fill) {
   ZKB_REQUIRE(!mats.empty(), "No matrices given");
-  if (h.field == FIELD_BABYBEAR && h.width == 16) return build_tree_impl<BabyBear, 16>(h, mats, tree, s, fri_layer, comb);
-  if (h.field == FIELD_GOLDILOCKS && h.width == 16) return build_tree_impl<Goldilocks, 16>(h, mats, tree, s, fri_layer, comb);
-  if (h.field == FIELD_GOLDILOCKS && h.width == 12) return build_tree_impl<Goldilocks, 12>(h, mats, tree, s, fri_layer, comb);
+  if (h.field == FIELD_BABYBEAR && h.width == 16) return build_tree_impl<BabyBear, 16>(h, mats, tree, s, fri_layer, comb, fill);
+  if (h.field == FIELD_GOLDILOCKS && h.width == 16) return build_tree_impl<Goldilocks, 16>(h, mats, tree, s, fri_layer, comb, fill);
+  if (h.field == FIELD_GOLDILOCKS && h.width == 12) return build_tree_impl<Goldilocks, 12>(h, mats, tree, s, fri_layer, comb, fill);
   set_error("unsupported hasher: field %d width %d", h.field, h.width);
   return ZKB_ERR_UNSUPPORTED;
+}
+
+int hash_rows_slab_dev(const HasherSpec &h, const uint32_t *mat, uint64_t stride, uint64_t c0, uint64_t ncols,
+                       uint64_t height, uint32_t *carry, bool first, bool last, uint32_t *digests,
+                       const LeafCombine *comb, cudaStream_t s) {
+  ZKB_REQUIRE(h.field == FIELD_BABYBEAR && h.width == 16, "internal: slab leaf hashing is BabyBear width 16");
+  ZKB_REQUIRE(c0 % 8 == 0 && (last || ncols % 8 == 0), "internal: slabs hold whole absorbed chunks");
+  P2Params<BabyBear, 16> p;
+  if (!build_p2_params<BabyBear, 16>(h, &p)) {
+    set_error("invalid Poseidon2 parameters");
+    return ZKB_ERR_INVALID;
+  }
+  const unsigned thr = 128;
+  ZKB_LAUNCH("merkle_leaf_hash", s, hash_rows_slab_kernel<<<grid_for(height, thr, 1u << 30), thr, 0, s>>>(mat, stride, c0, ncols, height, carry, first ? 1 : 0, last ? 1 : 0, digests, p, comb ? comb->apow : nullptr, comb ? comb->out : nullptr));
+  return ZKB_OK;
 }
 
 int mmcs_root_to_host(const DeviceTree *tree, void *root_out, cudaStream_t s) {

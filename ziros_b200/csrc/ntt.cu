@@ -471,14 +471,16 @@ static constexpr int pass_kmax() {
   return sizeof(typename F::T) == 4 ? 10 : 7;
 }
 
-// Runs the passes `ks` (bit counts, top first) starting at index bit hi_start.
+// Runs the passes `ks` (bit counts, top first) starting at index bit hi_start, over
+// `width` columns of a matrix whose rows are `stride` elements apart (0: width).
 template <class F>
 static int run_plan(const typename F::T *in, typename F::T *out, int L, uint32_t width,
                     uint64_t n_blocks, const typename F::T *tw, bool inverse,
                     typename F::T last_scale, const std::vector<int> &ks, int hi_start,
-                    cudaStream_t s, uint32_t cmax = 0) {
+                    cudaStream_t s, uint32_t cmax = 0, uint32_t stride = 0) {
   using T = typename F::T;
   if (cmax == 0) cmax = sizeof(T) == 4 ? 16 : 8;
+  if (stride == 0) stride = width;
   const std::vector<ColSeg> segs = col_segments(width, cmax);
   // the register DIFs use w_64 of the same direction as the table `tw`
   const SmallTw<F> st = small_twiddles<F>(inverse);
@@ -489,11 +491,11 @@ static int run_plan(const typename F::T *in, typename F::T *out, int L, uint32_t
     PassGeom g;
     g.L = L;
     g.lo = hi - K;
-    g.width = width;
+    g.width = stride;
     g.groups = 1u << (L - K);
-    g.block_stride = ((uint64_t)width) << L;
+    g.block_stride = ((uint64_t)stride) << L;
     g.twist = g.lo > 0;
-    if (((uint64_t)width << L) * n_blocks >= (1ull << 40)) {
+    if (((uint64_t)stride << L) * n_blocks >= (1ull << 40)) {
       set_error("NTT launch too large");
       return ZKB_ERR_UNSUPPORTED;
     }
@@ -735,13 +737,17 @@ int lde_tune_check(int field, uint32_t width, const LdeTune &t) {
 template <class F>
 int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log_b,
                 typename F::T shift, bool bitrev, typename F::T *d_out, cudaStream_t s,
-                const LdeTune *tune, typename F::T *coef_scratch) {
+                const LdeTune *tune, typename F::T *coef_scratch, uint32_t stride) {
   using T = typename F::T;
   if (width == 0) return ZKB_OK;
   if (log_h + log_b > F::TWO_ADICITY) {
     set_error("LDE size 2^%d exceeds the two-adicity of the field", log_h + log_b);
     return ZKB_ERR_INVALID;
   }
+  if (stride == 0) stride = width;
+  ZKB_REQUIRE(stride == width || (stride > width && bitrev && log_h > 0 && coef_scratch != nullptr),
+              "internal: an LDE of some columns of a wider matrix needs bit-reversed rows, a height above 1 "
+              "and a coefficient scratch of the same stride");
   LdeTune tn;
   if (tune) {
     ZKB_TRY(lde_tune_check(field_id<F>(), width, *tune));
@@ -769,12 +775,12 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
         cs = coef.as<T>();
       }
       std::vector<int> head(ks.begin(), ks.end() - 1);
-      ZKB_TRY(run_plan<F>(d_trace, cs, log_h, width, 1, itw, true, (T)0, head, log_h, s, tn.c_pass));
+      ZKB_TRY(run_plan<F>(d_trace, cs, log_h, width, 1, itw, true, (T)0, head, log_h, s, tn.c_pass, stride));
       src = cs;
     }
     FusedGeom g;
     g.L = log_h;
-    g.width = width;
+    g.width = stride;
     g.blocks = 1u << (log_h - Kf);
     g.log_b = log_b;
     g.n = n;
@@ -791,7 +797,7 @@ int ntt_lde_dev(const typename F::T *d_trace, int log_h, uint32_t width, int log
     std::vector<int> tail(ks.rbegin() + 1, ks.rend());
     if (!tail.empty())
       ZKB_TRY(run_plan<F>(d_out, d_out, log_h, width, 1ull << log_b, ftw, false, (T)0, tail,
-                          log_h - Kf, s, tn.c_pass));
+                          log_h - Kf, s, tn.c_pass, stride));
   }
   if (!bitrev) {
     const int LN = log_h + log_b;
@@ -844,9 +850,9 @@ template int get_twiddles<Goldilocks>(int, bool, const uint64_t **, cudaStream_t
 template int ntt_dft_dev<BabyBear>(uint32_t *, int, uint32_t, bool, cudaStream_t);
 template int ntt_dft_dev<Goldilocks>(uint64_t *, int, uint32_t, bool, cudaStream_t);
 template int ntt_lde_dev<BabyBear>(const uint32_t *, int, uint32_t, int, uint32_t, bool, uint32_t *,
-                                   cudaStream_t, const LdeTune *, uint32_t *);
+                                   cudaStream_t, const LdeTune *, uint32_t *, uint32_t);
 template int ntt_lde_dev<Goldilocks>(const uint64_t *, int, uint32_t, int, uint64_t, bool,
-                                     uint64_t *, cudaStream_t, const LdeTune *, uint64_t *);
+                                     uint64_t *, cudaStream_t, const LdeTune *, uint64_t *, uint32_t);
 
 void set_ntt_tile_loads(int mode) { ntt_tile_loads().store(mode); }
 int ntt_tile_loads_mode() { return ntt_tile_loads().load(); }

@@ -104,6 +104,8 @@ uint64_t job_bytes(const zkb_job_desc &d) {
   uint64_t b = n * d.width * es        // staged trace (the inverse passes run in place on it)
                + N * d.width * es      // LDE
                + 2 * N * 64;           // digest layers (upper bound)
+  // a trace uploaded in column slabs carries its rows' sponge states between slabs
+  if (d.hasher.field == ZKB_FIELD_BABYBEAR && d.hasher.width == 16 && d.width >= 128 && d.log_h >= 1) b += N * 64;
   if (d.with_fri) b += N * 16 + N * 64;  // codeword + FRI layers and trees
   return b + (64ull << 20);
 }
