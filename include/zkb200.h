@@ -282,7 +282,10 @@ ZKB_API int zkb_mmcs_compress(const zkb_hasher *hasher, const void *left, const 
  * bit-reversed, MMCS commit of the result — coset_lde_batch + bit_reverse_rows +
  * Mmcs::commit in one call.  The LDE (2^(log_h+log_blowup) x width) stays on the
  * device as the tree's leaf matrix, so openings read it without a copy.
- * Host form: `trace` is a host pointer (pinned memory gives full copy bandwidth). */
+ * Host form: `trace` is a host pointer (pinned memory gives full copy bandwidth).  A
+ * BabyBear trace of 128 or more columns (width-16 hasher) crosses the link a 64-column slab
+ * at a time, and each slab's LDE and leaf absorption run while the next slab is copied
+ * (the same for zkb_pcs_commit_fri and engine jobs); results are the device form's. */
 ZKB_API int zkb_pcs_commit(const zkb_hasher *hasher, const void *trace, uint32_t log_h,
                            uint32_t width, uint32_t log_blowup, void *root_out, zkb_tree **tree_out);
 ZKB_API int zkb_pcs_commit_dev(const zkb_hasher *hasher, const void *d_trace, uint32_t log_h,
