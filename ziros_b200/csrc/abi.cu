@@ -508,10 +508,13 @@ int pcs_commit_impl(const HasherSpec &spec, const void *d_trace, const void *h_t
     // else uploads every slab first and then waits for it, as an unslabbed job does.
     ScratchBuf carry;
     ZKB_TRY(carry.alloc(N * 16 * sizeof(uint32_t), s));
-    struct StreamHolder {
+    struct StreamHolder {  // on an early return, no copy may still write into the staged trace
       cudaStream_t c = nullptr;
       ~StreamHolder() {
-        if (c) cudaStreamDestroy(c);
+        if (c) {
+          cudaStreamSynchronize(c);
+          cudaStreamDestroy(c);
+        }
       }
     } cs;
     ZKB_CHECK_CUDA(cudaStreamCreateWithFlags(&cs.c, cudaStreamNonBlocking));
