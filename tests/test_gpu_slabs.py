@@ -71,3 +71,12 @@ def test_engine_slabbed_jobs_equal_device_path():
             _same_proof(p, pf)
     finally:
         eng.close()
+
+
+def test_pinned_host_commit_equals_device_commit():
+    t = rand_field(Z.BABYBEAR, (1 << 14, 192), 3300)
+    pinned = torch.from_numpy(t.view(np.int32)).pin_memory()
+    pcs = Z.CudaTwoAdicPcs(Z.BABYBEAR, 42, 1)
+    root_p, _ = pcs.commit_ptr(pinned.data_ptr(), 1 << 14, 192, want_tree=False)
+    root_d, _ = pcs.commit_dev(_dev(t), want_tree=False)
+    assert (root_p == root_d).all()
